@@ -1,0 +1,156 @@
+/*
+ * oneesan_fdp.h -- C ABI of the B200 frontier (transfer-matrix) DP engine.
+ *
+ * Counts simple corner-to-corner paths on an (n+1)x(n+1) vertex grid as uint32
+ * residues modulo primes below 2^32 (README.md:3 of the reference).  Every
+ * entry point takes plain pointers and sizes; device pointers are CUDA device
+ * addresses on the context's device, host pointers are ordinary memory.
+ *
+ * The reference's own boundary is a process (solver binary argv + one stdout
+ * line per modulus, GB.cu:2090-2101 and GB.cu:2257, with
+ * GB.cu = src/cuda/b300/oneesan_cuda_gridfp_b300_hbm32_factorized_fullprerank_orbit_blockfused_groupbatch_batch.cu).
+ * The CLI in this repository (oneesan_solver) keeps that contract and is
+ * itself a client of the functions below.  Each declaration names the
+ * reference interface it replaces.
+ *
+ * Conventions
+ *   - Status codes are returned, never exits or exceptions.  Codes 1-5 and 34
+ *     equal the reference solver's exit codes for the same condition
+ *     (GB.cu:2098-2184).
+ *   - One context per device; calls on one context are serialised by the
+ *     caller, except fdp_submit / fdp_poll, which are thread-safe.
+ *   - Residues are canonical in [0, p); moduli are in [2, 2^32 - 1].
+ *   - Coefficient vectors are in canonical rank order (GB.cu:1568 rank_full)
+ *     with `lanes` residues interleaved per state: word[state * lanes + l].
+ */
+#ifndef ONEESAN_FDP_H
+#define ONEESAN_FDP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fdp_status {
+  FDP_OK = 0,
+  FDP_ERR_ARGS = 1,         /* bad arguments (reference exit 1)                       */
+  FDP_ERR_GPU_COUNT = 2,    /* no usable GPU (reference exit 2)                       */
+  FDP_ERR_WINDOW = 4,       /* request does not fit the scratch/lanes limit (exit 4)  */
+  FDP_ERR_HBM = 5,          /* HBM budget or device memory exhausted (exit 5)         */
+  FDP_ERR_CUDA = 6,         /* a CUDA runtime error; see fdp_last_error()             */
+  FDP_ERR_MODULUS = 34,     /* modulus outside [2, 2^32-1] (reference exit 34 class)  */
+  FDP_PENDING = 100,        /* fdp_poll: request not finished yet                     */
+  FDP_TIMEOUT = 101,        /* a bounded wait ran out                                  */
+  FDP_ERR_NOT_FOUND = 102   /* unknown request slot                                    */
+} fdp_status;
+
+#define FDP_MAX_N 27      /* widest grid: W = n+1 <= 28 (GB.cu:28 MAXW)        */
+#define FDP_MAX_LANES 16  /* residues interleaved per state in one pass         */
+
+typedef struct fdp_ctx fdp_ctx;
+
+/* A problem: one grid size and a set of moduli. */
+typedef struct fdp_problem {
+  int n;                    /* grid cells per side, 1..27                         */
+  int k;                    /* number of moduli                                    */
+  const uint32_t *moduli;   /* k moduli (host memory)                              */
+  int lanes;                /* residues per pass: 1 = plain, k = batched (<=16)   */
+} fdp_problem;
+
+/* Memory and work plan of a problem (GRIDFP_PLAN_ONLY output, GB.cu:2117-2168). */
+typedef struct fdp_plan_out {
+  int n, width, k, lanes, passes;
+  int index_bits;                   /* 32 or 64                                   */
+  uint64_t main_states;             /* H_DP[W][1]                                 */
+  uint64_t blocked_states;          /* H_DP[W-1][1]                               */
+  uint64_t state_bytes;             /* 4 (M + D) lanes: the whole device footprint */
+  uint64_t scratch_bytes;           /* 0: the transition is in place              */
+  uint64_t table_bytes;             /* per-width index tables                     */
+  uint64_t total_bytes;
+  int rows;                         /* row sweeps per residue                     */
+  int cells_per_row;                /* W - 1                                      */
+  uint64_t alg_bytes_per_residue;   /* sum over cells of 4(M+D) + 4(Wm(p)+D)      */
+  uint64_t transitions_per_residue; /* sum over cells of (M + D)                  */
+  int fits;                         /* total_bytes <= budget                      */
+} fdp_plan_out;
+
+/* Per-call timing (the reference reports wall_s and phase sums, GB.cu:2257). */
+typedef struct fdp_run_stats {
+  double wall_s;          /* host wall clock of the whole call                   */
+  double device_s;        /* CUDA-event time of the captured sweep(s)             */
+  double capture_s;       /* graph capture + instantiate                          */
+  uint64_t kernel_launches;
+  uint64_t alg_bytes;     /* algorithmic bytes moved (all residues)               */
+  uint64_t transitions;   /* frontier transitions (all residues)                  */
+} fdp_run_stats;
+
+/* Library version string. */
+const char *fdp_version(void);
+/* Message of the last failing CUDA call on this thread ("" if none). */
+const char *fdp_last_error(void);
+
+/*
+ * Pure host planner, no device access.  Replaces GRIDFP_PLAN_ONLY=1
+ * (GB.cu:2117-2168) and the HBM admission check (GB.cu:2182-2186).
+ */
+fdp_status fdp_plan(const fdp_problem *problem, uint64_t hbm_budget_bytes, fdp_plan_out *out);
+
+/* Context on one device (replaces DeviceCtx::init and the allocations, GB.cu:2172-2186). */
+fdp_status fdp_create(fdp_ctx **out, int device);
+void fdp_destroy(fdp_ctx *ctx);
+
+/*
+ * Residues of the path count for every modulus of `problem`, synchronously.
+ * lanes = 1 runs one modulus per launch sequence (the reference's residue
+ * loop, GB.cu:2211-2258); lanes = k runs all moduli through one captured
+ * sweep with `lanes` residues per state.  residues_out has k entries.
+ */
+fdp_status fdp_run_sync(fdp_ctx *ctx, const fdp_problem *problem, uint32_t *residues_out, fdp_run_stats *stats);
+
+/*
+ * Operator level: apply cells p_hi, p_hi-1, ..., p_lo of one row sweep to
+ * caller-owned device vectors (width = n+1, main [M][lanes], block [D][lanes]).
+ * The blocked input is consumed at p_hi; the blocked output of p_lo is left in
+ * `block` (all zero when p_lo = 1).  Replaces process_window_batched_io for a
+ * window (GB.cu:1701-1742) as exercised by tests/groupbatch_operator_test.cu,
+ * and the reverse (pull) sweep kernels (R2.cu:1039-1155, R2.cu =
+ * src/cuda/b300/oneesan_cuda_gridfp_b300_hbm32_factorized_reverse2_row6crt20_batch.cu):
+ * this engine's cell operator is itself a pull sweep.  With all lane moduli
+ * equal, the lanes are independent vectors under one modulus, the GROUPBATCH
+ * lane semantics (src/cuda/b300/groupbatch_interleaved.cuh).
+ * `stream` is a cudaStream_t (0 = the context's stream); the call is async.
+ */
+fdp_status fdp_apply_cells(fdp_ctx *ctx, int width, int p_hi, int p_lo, int lanes, const uint32_t *moduli,
+                           uint32_t *d_main, uint32_t *d_block, void *stream);
+
+/*
+ * Profiling: run `rows` row sweeps of the problem's first pass (its first
+ * `lanes` moduli) on the context's resident state, each cell a separate launch
+ * bracketed by CUDA events on the context's stream, and return the mean
+ * duration of every cell p in cell_ms[p] (cell_ms has `width` entries, index
+ * 0 unused).  Values in the state are irrelevant to the timing: the kernel's
+ * access pattern depends only on indices.  Replaces the CUDA-event phase
+ * timers of GRIDFP_PROFILE_BATCH=1 (src/cuda/b300/factor_transfer_batch.cuh:110-158).
+ */
+fdp_status fdp_time_cells(fdp_ctx *ctx, const fdp_problem *problem, int rows, double *cell_ms);
+
+/* Canonical rank / unrank of frontier words on the device (GB.cu:1568 rank_full). */
+fdp_status fdp_rank_words(fdp_ctx *ctx, int width, const uint64_t *d_words, uint64_t *d_ranks, uint64_t count,
+                          void *stream);
+fdp_status fdp_unrank_words(fdp_ctx *ctx, int width, const uint64_t *d_ranks, uint64_t *d_words, uint64_t count,
+                            void *stream);
+
+/* Ternary rank index on the device (src/common/ternary_rank_index.hpp:6-15). */
+fdp_status fdp_ternary_index(fdp_ctx *ctx, const uint32_t *d_codes, uint32_t *d_index, uint64_t count, void *stream);
+
+/* Host helpers: state counts and the per-cell algorithmic byte model. */
+uint64_t fdp_main_states(int width);
+uint64_t fdp_blocked_states(int width);
+uint64_t fdp_cell_bytes(int width, int p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ONEESAN_FDP_H */

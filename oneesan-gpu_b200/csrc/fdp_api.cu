@@ -1,0 +1,314 @@
+// C ABI of the frontier-DP engine (include/oneesan_fdp.h).
+#include <chrono>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/oneesan_fdp.h"
+#include "fdp_api_internal.h"
+#include "fdp_host.h"
+#include "fdp_launch.h"
+
+using fdp::DevTables;
+
+static thread_local std::string g_last_error;
+
+static fdp_status cuda_status(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return FDP_OK;
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear a sticky-free error so the context stays usable
+  return e == cudaErrorMemoryAllocation ? FDP_ERR_HBM : FDP_ERR_CUDA;
+}
+
+#define FDP_CK(expr, what)                                  \
+  do {                                                      \
+    fdp_status _s = cuda_status((expr), (what));            \
+    if (_s != FDP_OK) return _s;                            \
+  } while (0)
+
+extern "C" const char *fdp_version(void) { return "oneesan-fdp-b200 0.1 (sm_100a)"; }
+extern "C" const char *fdp_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" uint64_t fdp_main_states(int width) { return fdp::main_states(width); }
+extern "C" uint64_t fdp_blocked_states(int width) { return fdp::blocked_states(width); }
+extern "C" uint64_t fdp_cell_bytes(int width, int p) {
+  if (width < 2 || width > FDP_MAXW || p < 1 || p >= width) return 0;
+  return fdp::cell_bytes(width, p);
+}
+
+static fdp_status check_problem(const fdp_problem *pr) {
+  if (!pr || pr->n < 1 || pr->n > FDP_MAX_N || pr->k < 1 || !pr->moduli) {
+    g_last_error = "problem: need 1 <= n <= 27, k >= 1 and a moduli array";
+    return FDP_ERR_ARGS;
+  }
+  if (pr->lanes < 1 || pr->lanes > FDP_MAX_LANES) {
+    g_last_error = "problem: lanes must be in 1..16";
+    return FDP_ERR_ARGS;
+  }
+  for (int i = 0; i < pr->k; ++i)
+    if (pr->moduli[i] < 2) {
+      g_last_error = "problem: modulus must be in [2, 2^32-1]";
+      return FDP_ERR_MODULUS;
+    }
+  return FDP_OK;
+}
+
+extern "C" fdp_status fdp_plan(const fdp_problem *pr, uint64_t budget, fdp_plan_out *out) {
+  fdp_status s = check_problem(pr);
+  if (s != FDP_OK) return s;
+  if (!out) return FDP_ERR_ARGS;
+  const int W = pr->n + 1;
+  const int lanes = pr->lanes < pr->k ? pr->lanes : pr->k;
+  fdp_plan_out o{};
+  o.n = pr->n;
+  o.width = W;
+  o.k = pr->k;
+  o.lanes = lanes;
+  o.passes = (pr->k + lanes - 1) / lanes;
+  o.index_bits = fdp::needs_u64(W) ? 64 : 32;
+  o.main_states = fdp::main_states(W);
+  o.blocked_states = fdp::blocked_states(W);
+  o.state_bytes = 4ull * (o.main_states + o.blocked_states) * uint64_t(lanes);
+  o.scratch_bytes = 0;
+  o.table_bytes = o.index_bits == 64 ? sizeof(fdp::WidthTables<uint64_t>) : sizeof(fdp::WidthTables<uint32_t>);
+  o.total_bytes = o.state_bytes + o.table_bytes + (1u << 20);
+  o.rows = fdp::sweep_rows(W);
+  o.cells_per_row = W - 1;
+  o.alg_bytes_per_residue = uint64_t(o.rows) * (W >= 2 ? fdp::row_bytes(W) : 0);
+  o.transitions_per_residue = uint64_t(o.rows) * uint64_t(o.cells_per_row) * fdp::cell_transitions(W);
+  o.fits = o.total_bytes <= budget ? 1 : 0;
+  *out = o;
+  return FDP_OK;
+}
+
+extern "C" fdp_status fdp_create(fdp_ctx **out, int device) {
+  if (!out) return FDP_ERR_ARGS;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) {
+    cudaGetLastError();
+    g_last_error = "no CUDA device visible";
+    return FDP_ERR_GPU_COUNT;
+  }
+  if (device < 0 || device >= count) {
+    g_last_error = "device index out of range";
+    return FDP_ERR_GPU_COUNT;
+  }
+  FDP_CK(cudaSetDevice(device), "cudaSetDevice");
+  auto *c = new fdp_ctx();
+  c->device = device;
+  fdp_status s = cuda_status(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+  if (s == FDP_OK) s = cuda_status(cudaMalloc(&c->d_acc, sizeof(unsigned long long) * FDP_MAX_LANES), "acc");
+  if (s == FDP_OK) s = cuda_status(cudaMalloc(&c->d_res, sizeof(uint32_t) * FDP_MAX_LANES), "res");
+  if (s == FDP_OK) s = cuda_status(cudaMallocHost(&c->h_res, sizeof(uint32_t) * FDP_MAX_LANES), "pinned res");
+  if (s == FDP_OK) s = cuda_status(cudaEventCreate(&c->ev0), "event");
+  if (s == FDP_OK) s = cuda_status(cudaEventCreate(&c->ev1), "event");
+  if (s != FDP_OK) {
+    fdp_destroy(c);
+    return s;
+  }
+  *out = c;
+  return FDP_OK;
+}
+
+fdp_ctx::~fdp_ctx() {
+  cudaSetDevice(device);
+  if (stream) cudaStreamSynchronize(stream);
+  for (auto &kv : tables) fdp::free_tables(&kv.second);
+  if (d_main) cudaFree(d_main);
+  if (d_blk) cudaFree(d_blk);
+  if (d_acc) cudaFree(d_acc);
+  if (d_res) cudaFree(d_res);
+  if (h_res) cudaFreeHost(h_res);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+extern "C" void fdp_destroy(fdp_ctx *ctx) { delete ctx; }
+
+fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const DevTables **out) {
+  auto it = c->tables.find(W);
+  if (it == c->tables.end()) {
+    DevTables t;
+    FDP_CK(fdp::upload_tables(W, &t), "upload tables");
+    it = c->tables.emplace(W, t).first;
+  }
+  *out = &it->second;
+  return FDP_OK;
+}
+
+static fdp_status ensure_buffer(uint32_t **buf, size_t *cap, size_t bytes, const char *what) {
+  if (*cap >= bytes && *buf) return FDP_OK;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  FDP_CK(cudaMalloc(buf, bytes ? bytes : 4), what);
+  *cap = bytes;
+  return FDP_OK;
+}
+
+// Enqueue one whole residue pass (zero, row-0 init, row sweeps, dot product,
+// residue copy to pinned host memory) on `s`.
+fdp_status fdp_enqueue_pass(fdp_ctx *c, const DevTables &t, int L, const uint32_t *mods, uint32_t *main,
+                            uint32_t *blk, unsigned long long *acc, uint32_t *d_res, uint32_t *h_res,
+                            cudaStream_t s, uint64_t *launches) {
+  const int W = t.W;
+  const uint64_t M = fdp::main_states(W);
+  FDP_CK(cudaMemsetAsync(main, 0, size_t(M) * L * 4, s), "zero main");
+  FDP_CK(fdp::launch_first_row_init(t, L, main, s), "row-0 init");
+  uint64_t n = 1;
+  for (int row = 1; row <= fdp::sweep_rows(W); ++row)
+    for (int p = W - 1; p >= 1; --p) {
+      FDP_CK(fdp::launch_cell(t, L, mods, main, blk, p, p == W - 1, false, c->cfg, s), "cell");
+      ++n;
+    }
+  FDP_CK(fdp::launch_first_row_dot(t, L, mods, main, acc, d_res, s), "first-row dot");
+  n += 2;
+  if (h_res) FDP_CK(cudaMemcpyAsync(h_res, d_res, sizeof(uint32_t) * L, cudaMemcpyDeviceToHost, s), "residue copy");
+  if (launches) *launches += n;
+  return FDP_OK;
+}
+
+extern "C" fdp_status fdp_run_sync(fdp_ctx *c, const fdp_problem *pr, uint32_t *residues_out, fdp_run_stats *st) {
+  if (!c || !residues_out) return FDP_ERR_ARGS;
+  fdp_status s = check_problem(pr);
+  if (s != FDP_OK) return s;
+  std::lock_guard<std::mutex> lk(c->mu);
+  auto t0 = std::chrono::steady_clock::now();
+  FDP_CK(cudaSetDevice(c->device), "cudaSetDevice");
+  const int W = pr->n + 1;
+  const DevTables *t = nullptr;
+  if ((s = fdp_ctx_tables(c, W, &t)) != FDP_OK) return s;
+  const int lanes = pr->lanes < pr->k ? pr->lanes : pr->k;
+  const uint64_t M = fdp::main_states(W), D = fdp::blocked_states(W);
+  if ((s = ensure_buffer(&c->d_main, &c->cap_main, size_t(M) * lanes * 4, "main state")) != FDP_OK) return s;
+  if ((s = ensure_buffer(&c->d_blk, &c->cap_blk, size_t(D) * lanes * 4, "blocked state")) != FDP_OK) return s;
+  fdp_run_stats acc{};
+  for (int done = 0; done < pr->k; done += lanes) {
+    const int L = (pr->k - done) < lanes ? (pr->k - done) : lanes;
+    const uint32_t *mods = pr->moduli + done;
+    auto c0 = std::chrono::steady_clock::now();
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    FDP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    uint64_t launches = 0;
+    fdp_status es = fdp_enqueue_pass(c, *t, L, mods, c->d_main, c->d_blk, c->d_acc, c->d_res, c->h_res,
+                                     c->stream, &launches);
+    cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+    if (es != FDP_OK) {
+      if (g) cudaGraphDestroy(g);
+      return es;
+    }
+    FDP_CK(ce, "end capture");
+    ce = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    FDP_CK(ce, "graph instantiate");
+    acc.capture_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - c0).count();
+    cudaEventRecord(c->ev0, c->stream);
+    ce = cudaGraphLaunch(ge, c->stream);
+    cudaEventRecord(c->ev1, c->stream);
+    cudaError_t se = cudaStreamSynchronize(c->stream);
+    cudaGraphExecDestroy(ge);
+    FDP_CK(ce, "graph launch");
+    FDP_CK(se, "residue pass");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    acc.device_s += ms * 1e-3;
+    acc.kernel_launches += launches;
+    for (int i = 0; i < L; ++i) residues_out[done + i] = c->h_res[i];
+  }
+  fdp_plan_out po{};
+  fdp_plan(pr, ~0ull, &po);
+  acc.alg_bytes = po.alg_bytes_per_residue * uint64_t(pr->k);
+  acc.transitions = po.transitions_per_residue * uint64_t(pr->k);
+  acc.wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (st) *st = acc;
+  return FDP_OK;
+}
+
+extern "C" fdp_status fdp_apply_cells(fdp_ctx *c, int width, int p_hi, int p_lo, int lanes, const uint32_t *moduli,
+                                      uint32_t *d_main, uint32_t *d_block, void *stream) {
+  if (!c || !moduli || !d_main || !d_block) return FDP_ERR_ARGS;
+  if (width < 2 || width > FDP_MAXW || p_lo < 1 || p_hi >= width || p_lo > p_hi || lanes < 1 ||
+      lanes > FDP_MAX_LANES) {
+    g_last_error = "apply_cells: need 2 <= width <= 28, 1 <= p_lo <= p_hi < width, 1 <= lanes <= 16";
+    return FDP_ERR_ARGS;
+  }
+  for (int i = 0; i < lanes; ++i)
+    if (moduli[i] < 2) return FDP_ERR_MODULUS;
+  std::lock_guard<std::mutex> lk(c->mu);
+  FDP_CK(cudaSetDevice(c->device), "cudaSetDevice");
+  const DevTables *t = nullptr;
+  fdp_status s = fdp_ctx_tables(c, width, &t);
+  if (s != FDP_OK) return s;
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  for (int p = p_hi; p >= p_lo; --p)
+    FDP_CK(fdp::launch_cell(*t, lanes, moduli, d_main, d_block, p, false, true, c->cfg, st), "cell");
+  return FDP_OK;
+}
+
+extern "C" fdp_status fdp_rank_words(fdp_ctx *c, int width, const uint64_t *d_words, uint64_t *d_ranks,
+                                     uint64_t count, void *stream) {
+  if (!c || width < 1 || width > FDP_MAXW || (count && (!d_words || !d_ranks))) return FDP_ERR_ARGS;
+  FDP_CK(cudaSetDevice(c->device), "cudaSetDevice");
+  FDP_CK(fdp::launch_rank_words(width, d_words, d_ranks, count, stream ? (cudaStream_t)stream : c->stream), "rank");
+  return FDP_OK;
+}
+
+extern "C" fdp_status fdp_unrank_words(fdp_ctx *c, int width, const uint64_t *d_ranks, uint64_t *d_words,
+                                       uint64_t count, void *stream) {
+  if (!c || width < 1 || width > FDP_MAXW || (count && (!d_words || !d_ranks))) return FDP_ERR_ARGS;
+  FDP_CK(cudaSetDevice(c->device), "cudaSetDevice");
+  FDP_CK(fdp::launch_unrank_words(width, d_ranks, d_words, count, stream ? (cudaStream_t)stream : c->stream),
+         "unrank");
+  return FDP_OK;
+}
+
+extern "C" fdp_status fdp_ternary_index(fdp_ctx *c, const uint32_t *d_codes, uint32_t *d_index, uint64_t count,
+                                        void *stream) {
+  if (!c || (count && (!d_codes || !d_index))) return FDP_ERR_ARGS;
+  FDP_CK(cudaSetDevice(c->device), "cudaSetDevice");
+  FDP_CK(fdp::launch_ternary_index(d_codes, d_index, count, stream ? (cudaStream_t)stream : c->stream), "ternary");
+  return FDP_OK;
+}
+
+extern "C" fdp_status fdp_time_cells(fdp_ctx *c, const fdp_problem *pr, int rows, double *cell_ms) {
+  if (!c || !cell_ms || rows < 1) return FDP_ERR_ARGS;
+  fdp_status s = check_problem(pr);
+  if (s != FDP_OK) return s;
+  std::lock_guard<std::mutex> lk(c->mu);
+  FDP_CK(cudaSetDevice(c->device), "cudaSetDevice");
+  const int W = pr->n + 1;
+  if (W < 3) return FDP_ERR_ARGS;
+  const DevTables *t = nullptr;
+  if ((s = fdp_ctx_tables(c, W, &t)) != FDP_OK) return s;
+  const int L = pr->lanes < pr->k ? pr->lanes : pr->k;
+  const uint64_t M = fdp::main_states(W), D = fdp::blocked_states(W);
+  if ((s = ensure_buffer(&c->d_main, &c->cap_main, size_t(M) * L * 4, "main state")) != FDP_OK) return s;
+  if ((s = ensure_buffer(&c->d_blk, &c->cap_blk, size_t(D) * L * 4, "blocked state")) != FDP_OK) return s;
+  std::vector<cudaEvent_t> ev(size_t(rows) * W * 2);
+  for (auto &e : ev) FDP_CK(cudaEventCreate(&e), "event");
+  fdp_status rs = FDP_OK;
+  for (int r = 0; r < rows && rs == FDP_OK; ++r)
+    for (int p = W - 1; p >= 1 && rs == FDP_OK; --p) {
+      cudaEventRecord(ev[(size_t(r) * W + p) * 2], c->stream);
+      rs = cuda_status(fdp::launch_cell(*t, L, pr->moduli, c->d_main, c->d_blk, p, p == W - 1, false, c->cfg,
+                                        c->stream), "cell");
+      cudaEventRecord(ev[(size_t(r) * W + p) * 2 + 1], c->stream);
+    }
+  cudaError_t se = cudaStreamSynchronize(c->stream);
+  if (rs == FDP_OK) rs = cuda_status(se, "timed cells");
+  if (rs == FDP_OK) {
+    for (int p = 0; p < W; ++p) cell_ms[p] = 0;
+    for (int r = 0; r < rows; ++r)
+      for (int p = W - 1; p >= 1; --p) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev[(size_t(r) * W + p) * 2], ev[(size_t(r) * W + p) * 2 + 1]);
+        cell_ms[p] += ms / rows;
+      }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  return rs;
+}

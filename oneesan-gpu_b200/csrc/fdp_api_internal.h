@@ -1,0 +1,30 @@
+// Context object behind the opaque fdp_ctx handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+
+#include "../../include/oneesan_fdp.h"
+#include "fdp_launch.h"
+
+struct fdp_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::map<int, fdp::DevTables> tables;  // per frontier width
+  uint32_t *d_main = nullptr;            // run_sync state, [M][lanes]
+  uint32_t *d_blk = nullptr;             // run_sync state, [D][lanes]
+  size_t cap_main = 0, cap_blk = 0;
+  unsigned long long *d_acc = nullptr;   // first-row dot accumulators
+  uint32_t *d_res = nullptr;             // residues on the device
+  uint32_t *h_res = nullptr;             // residues, pinned host
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  fdp::LaunchCfg cfg;
+  std::mutex mu;
+  ~fdp_ctx();
+};
+
+fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const fdp::DevTables **out);
+fdp_status fdp_enqueue_pass(fdp_ctx *c, const fdp::DevTables &t, int L, const uint32_t *mods, uint32_t *main,
+                            uint32_t *blk, unsigned long long *acc, uint32_t *d_res, uint32_t *h_res,
+                            cudaStream_t s, uint64_t *launches);

@@ -1,0 +1,49 @@
+// Host-side tables, sizes and the byte model of the frontier DP.
+#pragma once
+#include <stdint.h>
+#include <vector>
+
+#include "fdp_core.cuh"
+
+namespace fdp {
+
+// H[w][h] in 64 bits for every width up to FDP_MAXW (GB.cu:172 build_full_dp).
+struct CountTable {
+  uint64_t H[FDP_MAXW + 1][FDP_HT];
+  CountTable();
+  uint64_t at(int w, int h) const { return (w < 0 || h < 0 || h >= FDP_HT || w > FDP_MAXW) ? 0 : H[w][h]; }
+};
+const CountTable &counts();
+
+uint64_t main_states(int W);     // H[W][1]
+uint64_t blocked_states(int W);  // H[W-1][1]
+
+// Index width needed for a frontier of width W: main ranks must fit the type.
+bool needs_u64(int W);
+
+// Fill the device table blob for width W.
+template <typename Idx>
+void build_width_tables(int W, WidthTables<Idx> *out);
+
+// Canonical rank / unrank (host reference of the device routines).
+uint64_t rank_word(uint64_t word, int width);
+uint64_t unrank_word(uint64_t rank, int width);
+
+// The state reached by one first-row edge mask (GB.cu:1081-1096).
+uint64_t first_row_state(uint64_t mask, int W);
+
+// include_horizontal (TR.hpp:113-144): 0 invalid, 1 main, 2 blocked.
+int include_horizontal(uint64_t m, int width, int p, uint64_t *out);
+
+// Algorithmic bytes of one cell p for one modulus:
+//   4(M+D) + 4(Wm(p)+D), Wm(p) = main targets that can change (p=1: all).
+uint64_t cell_bytes(int W, int p);
+// Algorithmic bytes of one full row sweep p = W-1..1, one modulus.
+uint64_t row_bytes(int W);
+// Frontier transitions of one cell (main + blocked states), one modulus.
+uint64_t cell_transitions(int W);
+
+// Number of row sweeps a residue runs with the row-0 initialiser (prefixK = 1).
+inline int sweep_rows(int W) { return W >= 3 ? W - 2 : 0; }
+
+}  // namespace fdp

@@ -1,0 +1,100 @@
+// Explicit instantiations of the cell / first-row kernels for K in
+// [FDP_K_LO, FDP_K_HI]; the build compiles this file once per K range so the
+// 2 x 16 kernel variants build in parallel.
+#include "fdp_kernels.cuh"
+#include "fdp_launch.h"
+
+#ifndef FDP_K_LO
+#define FDP_K_LO 1
+#endif
+#ifndef FDP_K_HI
+#define FDP_K_HI 16
+#endif
+
+namespace fdp {
+
+template <typename Idx, int K>
+cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t s) {
+  int grid = cfg.grid;
+  if (grid <= 0) {
+    static int per_sm = 0;  // resident CTAs per SM for this variant
+    if (!per_sm) {
+      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cell_kernel<Idx, K>, cfg.block, 0);
+      if (e != cudaSuccess) return e;
+      if (per_sm < 1) per_sm = 1;
+    }
+    grid = device_sm_count() * per_sm;
+  }
+  const uint64_t need = (a.items + cfg.block - 1) / cfg.block;
+  if (uint64_t(grid) > need) grid = int(need ? need : 1);
+  cell_kernel<Idx, K><<<grid, cfg.block, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename Idx, int K>
+cudaError_t launch_first_row_t(const FirstRowArgs &a, bool dot, cudaStream_t s) {
+  const uint64_t total = 1ull << (a.W - 1);
+  uint64_t blocks = (total + 255) / 256;
+  const uint64_t cap = uint64_t(device_sm_count()) * 8;
+  if (blocks > cap) blocks = cap;
+  if (dot) first_row_dot_kernel<Idx, K><<<unsigned(blocks), 256, 0, s>>>(a);
+  else first_row_init_kernel<Idx, K><<<unsigned(blocks), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+#define FDP_INST(K)                                                                              \
+  template cudaError_t launch_cell_t<uint32_t, K>(const CellArgs &, const LaunchCfg &, cudaStream_t); \
+  template cudaError_t launch_cell_t<uint64_t, K>(const CellArgs &, const LaunchCfg &, cudaStream_t); \
+  template cudaError_t launch_first_row_t<uint32_t, K>(const FirstRowArgs &, bool, cudaStream_t);    \
+  template cudaError_t launch_first_row_t<uint64_t, K>(const FirstRowArgs &, bool, cudaStream_t);
+
+#if FDP_K_LO <= 1 && 1 <= FDP_K_HI
+FDP_INST(1)
+#endif
+#if FDP_K_LO <= 2 && 2 <= FDP_K_HI
+FDP_INST(2)
+#endif
+#if FDP_K_LO <= 3 && 3 <= FDP_K_HI
+FDP_INST(3)
+#endif
+#if FDP_K_LO <= 4 && 4 <= FDP_K_HI
+FDP_INST(4)
+#endif
+#if FDP_K_LO <= 5 && 5 <= FDP_K_HI
+FDP_INST(5)
+#endif
+#if FDP_K_LO <= 6 && 6 <= FDP_K_HI
+FDP_INST(6)
+#endif
+#if FDP_K_LO <= 7 && 7 <= FDP_K_HI
+FDP_INST(7)
+#endif
+#if FDP_K_LO <= 8 && 8 <= FDP_K_HI
+FDP_INST(8)
+#endif
+#if FDP_K_LO <= 9 && 9 <= FDP_K_HI
+FDP_INST(9)
+#endif
+#if FDP_K_LO <= 10 && 10 <= FDP_K_HI
+FDP_INST(10)
+#endif
+#if FDP_K_LO <= 11 && 11 <= FDP_K_HI
+FDP_INST(11)
+#endif
+#if FDP_K_LO <= 12 && 12 <= FDP_K_HI
+FDP_INST(12)
+#endif
+#if FDP_K_LO <= 13 && 13 <= FDP_K_HI
+FDP_INST(13)
+#endif
+#if FDP_K_LO <= 14 && 14 <= FDP_K_HI
+FDP_INST(14)
+#endif
+#if FDP_K_LO <= 15 && 15 <= FDP_K_HI
+FDP_INST(15)
+#endif
+#if FDP_K_LO <= 16 && 16 <= FDP_K_HI
+FDP_INST(16)
+#endif
+
+}  // namespace fdp

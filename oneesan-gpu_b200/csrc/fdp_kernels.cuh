@@ -1,0 +1,89 @@
+// sm_100a kernels of the frontier DP: the per-cell transition (pull form, in
+// place, no atomics), the row-0 initialiser and the first-row dot product.
+// The per-item arithmetic lives in fdp_item.cuh.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fdp_item.cuh"
+
+namespace fdp {
+
+template <typename Idx>
+__device__ __forceinline__ void load_cell_smem(CellSmem<Idx> &sm, const WidthTables<Idx> *t, int W, int p) {
+  const int nthr = blockDim.x, tid = threadIdx.x;
+  for (int i = tid; i < (FDP_MAXW + 1) * FDP_HT; i += nthr) (&sm.H[0][0])[i] = (&t->H[0][0])[i];
+  // Only blocked positions p..W-2 are walked by the prefix decode.
+  const int rows = W - 1 - p;
+  for (int i = tid; i < rows * FDP_HT; i += nthr) {
+    const int pos = p + i / FDP_HT, h = i % FDP_HT;
+    sm.S[pos][h] = t->S[pos][h];
+  }
+  for (int i = tid; i < FDP_HT * PR_COUNT; i += nthr) (&sm.OFF[0][0])[i] = (&t->OFF[p][0][0])[i];
+}
+
+template <typename Idx, int K>
+__global__ void __launch_bounds__(256) cell_kernel(const CellArgs a) {
+  __shared__ CellSmem<Idx> sm;
+  load_cell_smem<Idx>(sm, reinterpret_cast<const WidthTables<Idx> *>(a.tables), a.W, a.p);
+  __syncthreads();
+  const Idx n = Idx(a.items);
+  const Idx stride = Idx(gridDim.x) * blockDim.x;
+  for (Idx j = Idx(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride) cell_item<Idx, K>(a, sm, j);
+}
+
+template <typename Idx, int K>
+__global__ void __launch_bounds__(256) first_row_init_kernel(const FirstRowArgs a) {
+  __shared__ Idx sH[FDP_MAXW + 1][FDP_HT];
+  const WidthTables<Idx> *t = reinterpret_cast<const WidthTables<Idx> *>(a.tables);
+  for (int i = threadIdx.x; i < (FDP_MAXW + 1) * FDP_HT; i += blockDim.x) (&sH[0][0])[i] = (&t->H[0][0])[i];
+  __syncthreads();
+  const uint64_t total = 1ull << (a.W - 1);
+  uint32_t one[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) one[i] = 1u;
+  for (uint64_t mask = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; mask < total;
+       mask += uint64_t(gridDim.x) * blockDim.x) {
+    const Idx rk = rank_dev<Idx>(first_row_state_dev(mask, a.W), a.W, sH);
+    stk<K>(a.main + size_t(rk) * K, one);
+  }
+}
+
+template <typename Idx, int K>
+__global__ void __launch_bounds__(256) first_row_dot_kernel(const FirstRowArgs a) {
+  __shared__ Idx sH[FDP_MAXW + 1][FDP_HT];
+  __shared__ unsigned long long red[8][K];
+  const WidthTables<Idx> *t = reinterpret_cast<const WidthTables<Idx> *>(a.tables);
+  for (int i = threadIdx.x; i < (FDP_MAXW + 1) * FDP_HT; i += blockDim.x) (&sH[0][0])[i] = (&t->H[0][0])[i];
+  __syncthreads();
+  const uint64_t total = 1ull << (a.W - 1);
+  unsigned long long acc[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) acc[i] = 0;
+  for (uint64_t mask = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; mask < total;
+       mask += uint64_t(gridDim.x) * blockDim.x) {
+    const Idx rk = rank_dev<Idx>(first_row_state_dev(mask, a.W), a.W, sH);
+    uint32_t v[K];
+    ldk<K>(a.main + size_t(rk) * K, v);
+#pragma unroll
+    for (int i = 0; i < K; ++i) acc[i] += v[i];
+  }
+  // Exact 64-bit sums: at most 2^27 terms below 2^32 each.
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    unsigned long long v = acc[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][i] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < K) {
+    unsigned long long v = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
+    atomicAdd(a.acc + threadIdx.x, v);
+  }
+}
+
+// residue[k] = acc[k] mod p_k
+__global__ void finalize_residues_kernel(const unsigned long long *acc, uint32_t *out, FirstRowArgs a, int k);
+
+}  // namespace fdp

@@ -1,0 +1,48 @@
+// Host-side launchers for the frontier-DP kernels (dispatch on index width and
+// on K = residues interleaved per state).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fdp_item.cuh"
+
+namespace fdp {
+
+constexpr int kMaxLanes = 16;  // K = 1..16 residues interleaved per state
+
+// Per-width device table blob.
+struct DevTables {
+  void *ptr = nullptr;
+  bool u64 = false;
+  int W = 0;
+};
+cudaError_t upload_tables(int W, DevTables *out);
+void free_tables(DevTables *t);
+
+struct LaunchCfg {
+  int block = 256;
+  int grid = 0;  // 0: sized from occupancy (a multiple of the SM count)
+};
+
+template <typename Idx, int K>
+cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t s);
+template <typename Idx, int K>
+cudaError_t launch_first_row_t(const FirstRowArgs &a, bool dot, cudaStream_t s);
+
+// One cell p on [M][K] / [D][K] arrays.
+cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_t *main, uint32_t *blk, int p,
+                        bool blk_in_zero, bool blk_out_p1, const LaunchCfg &cfg, cudaStream_t s);
+// main[rank(first-row state)] = 1 for every first-row mask.
+cudaError_t launch_first_row_init(const DevTables &t, int K, uint32_t *main, cudaStream_t s);
+// acc[k] += sum over first-row states of main[.][k]; then residues[k] = acc[k] mod p_k.
+cudaError_t launch_first_row_dot(const DevTables &t, int K, const uint32_t *mods, const uint32_t *main,
+                                 unsigned long long *acc, uint32_t *residues, cudaStream_t s);
+
+// Operator-surface helpers.
+cudaError_t launch_rank_words(int width, const uint64_t *words, uint64_t *ranks, uint64_t count, cudaStream_t s);
+cudaError_t launch_unrank_words(int width, const uint64_t *ranks, uint64_t *words, uint64_t count, cudaStream_t s);
+cudaError_t launch_ternary_index(const uint32_t *codes, uint32_t *index, uint64_t count, cudaStream_t s);
+
+int device_sm_count();
+
+}  // namespace fdp

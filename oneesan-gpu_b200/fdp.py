@@ -1,0 +1,183 @@
+"""ctypes binding of libfdp.so, the C ABI in include/oneesan_fdp.h.
+
+This is the Python face of the engine used by the tests and bench.py.  It has
+no compute of its own: every call goes through libfdp.so, and loading fails
+loudly if the library has not been built (``make -C oneesan-gpu_b200``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import Sequence
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfdp.so")
+
+FDP_OK = 0
+FDP_ERR_ARGS = 1
+FDP_ERR_GPU_COUNT = 2
+FDP_ERR_WINDOW = 4
+FDP_ERR_HBM = 5
+FDP_ERR_CUDA = 6
+FDP_ERR_MODULUS = 34
+FDP_PENDING = 100
+FDP_TIMEOUT = 101
+FDP_ERR_NOT_FOUND = 102
+MAX_LANES = 16
+MAX_N = 27
+
+
+class FdpError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{where}: fdp status {status} {detail}".strip())
+
+
+class Problem(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("k", ctypes.c_int),
+                ("moduli", ctypes.POINTER(ctypes.c_uint32)), ("lanes", ctypes.c_int)]
+
+
+class PlanOut(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("width", ctypes.c_int), ("k", ctypes.c_int),
+                ("lanes", ctypes.c_int), ("passes", ctypes.c_int), ("index_bits", ctypes.c_int),
+                ("main_states", ctypes.c_uint64), ("blocked_states", ctypes.c_uint64),
+                ("state_bytes", ctypes.c_uint64), ("scratch_bytes", ctypes.c_uint64),
+                ("table_bytes", ctypes.c_uint64), ("total_bytes", ctypes.c_uint64),
+                ("rows", ctypes.c_int), ("cells_per_row", ctypes.c_int),
+                ("alg_bytes_per_residue", ctypes.c_uint64),
+                ("transitions_per_residue", ctypes.c_uint64), ("fits", ctypes.c_int)]
+
+
+class RunStats(ctypes.Structure):
+    _fields_ = [("wall_s", ctypes.c_double), ("device_s", ctypes.c_double),
+                ("capture_s", ctypes.c_double), ("kernel_launches", ctypes.c_uint64),
+                ("alg_bytes", ctypes.c_uint64), ("transitions", ctypes.c_uint64)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libfdp.so once; raise if it is missing (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libfdp.so not built at {LIB_PATH}; run `make -C oneesan-gpu_b200`")
+    L = ctypes.CDLL(LIB_PATH)
+    c_int, c_u32, c_u64, c_vp = ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p
+    P = ctypes.POINTER
+    L.fdp_version.restype = ctypes.c_char_p
+    L.fdp_last_error.restype = ctypes.c_char_p
+    L.fdp_plan.argtypes = [P(Problem), c_u64, P(PlanOut)]
+    L.fdp_create.argtypes = [P(c_vp), c_int]
+    L.fdp_destroy.argtypes = [c_vp]
+    L.fdp_destroy.restype = None
+    L.fdp_run_sync.argtypes = [c_vp, P(Problem), P(c_u32), P(RunStats)]
+    L.fdp_apply_cells.argtypes = [c_vp, c_int, c_int, c_int, c_int, P(c_u32), c_vp, c_vp, c_vp]
+    L.fdp_time_cells.argtypes = [c_vp, P(Problem), c_int, P(ctypes.c_double)]
+    L.fdp_rank_words.argtypes = [c_vp, c_int, c_vp, c_vp, c_u64, c_vp]
+    L.fdp_unrank_words.argtypes = [c_vp, c_int, c_vp, c_vp, c_u64, c_vp]
+    L.fdp_ternary_index.argtypes = [c_vp, c_vp, c_vp, c_u64, c_vp]
+    for name in ("fdp_main_states", "fdp_blocked_states"):
+        getattr(L, name).argtypes = [c_int]
+        getattr(L, name).restype = c_u64
+    L.fdp_cell_bytes.argtypes = [c_int, c_int]
+    L.fdp_cell_bytes.restype = c_u64
+    _lib = L
+    return L
+
+
+def _check(status: int, where: str) -> None:
+    if status != FDP_OK:
+        detail = lib().fdp_last_error().decode(errors="replace")
+        raise FdpError(status, where, detail)
+
+
+def _u32_array(values: Sequence[int]):
+    return (ctypes.c_uint32 * len(values))(*[int(v) for v in values])
+
+
+def main_states(width: int) -> int:
+    return int(lib().fdp_main_states(width))
+
+
+def blocked_states(width: int) -> int:
+    return int(lib().fdp_blocked_states(width))
+
+
+def cell_bytes(width: int, p: int) -> int:
+    return int(lib().fdp_cell_bytes(width, p))
+
+
+def plan(n: int, moduli: Sequence[int], lanes: int | None = None, budget: int = 1 << 62) -> PlanOut:
+    mods = _u32_array(moduli)
+    pr = Problem(n, len(moduli), mods, lanes or min(len(moduli), MAX_LANES))
+    out = PlanOut()
+    _check(lib().fdp_plan(ctypes.byref(pr), budget, ctypes.byref(out)), "fdp_plan")
+    return out
+
+
+@dataclass
+class Result:
+    residues: list
+    stats: RunStats
+
+
+class Engine:
+    """One engine context on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self._ctx = ctypes.c_void_p()
+        _check(lib().fdp_create(ctypes.byref(self._ctx), device), "fdp_create")
+
+    def close(self) -> None:
+        if self._ctx:
+            lib().fdp_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def residues(self, n: int, moduli: Sequence[int], lanes: int | None = None) -> Result:
+        """Residues of the corner-path count of the n x n grid, one per modulus."""
+        mods = _u32_array(moduli)
+        pr = Problem(n, len(moduli), mods, lanes or min(len(moduli), MAX_LANES))
+        out = (ctypes.c_uint32 * len(moduli))()
+        st = RunStats()
+        _check(lib().fdp_run_sync(self._ctx, ctypes.byref(pr), out, ctypes.byref(st)), "fdp_run_sync")
+        return Result([int(x) for x in out], st)
+
+    def time_cells(self, n: int, moduli: Sequence[int], lanes: int | None = None, rows: int = 1) -> list:
+        """Mean CUDA-event duration (ms) of each cell p = 1..n of a row sweep; index 0 unused."""
+        mods = _u32_array(moduli)
+        pr = Problem(n, len(moduli), mods, lanes or min(len(moduli), MAX_LANES))
+        out = (ctypes.c_double * (n + 1))()
+        _check(lib().fdp_time_cells(self._ctx, ctypes.byref(pr), rows, out), "fdp_time_cells")
+        return [float(x) for x in out]
+
+    def apply_cells(self, width: int, p_hi: int, p_lo: int, moduli: Sequence[int], main_ptr: int,
+                    block_ptr: int, stream: int = 0) -> None:
+        mods = _u32_array(moduli)
+        _check(lib().fdp_apply_cells(self._ctx, width, p_hi, p_lo, len(moduli), mods, main_ptr, block_ptr,
+                                     stream), "fdp_apply_cells")
+
+    def rank_words(self, width: int, words_ptr: int, ranks_ptr: int, count: int, stream: int = 0) -> None:
+        _check(lib().fdp_rank_words(self._ctx, width, words_ptr, ranks_ptr, count, stream), "fdp_rank_words")
+
+    def unrank_words(self, width: int, ranks_ptr: int, words_ptr: int, count: int, stream: int = 0) -> None:
+        _check(lib().fdp_unrank_words(self._ctx, width, ranks_ptr, words_ptr, count, stream), "fdp_unrank_words")
+
+    def ternary_index(self, codes_ptr: int, index_ptr: int, count: int, stream: int = 0) -> None:
+        _check(lib().fdp_ternary_index(self._ctx, codes_ptr, index_ptr, count, stream), "fdp_ternary_index")

@@ -1,0 +1,51 @@
+"""End-to-end residues through the C ABI (fdp_run_sync) against the oracle, the
+reference's published residues and exact counts reconstructed by CRT."""
+import pytest
+
+import oracle_lib as orc
+
+pytestmark = pytest.mark.gpu
+
+P = orc.largest_primes_below_2_32(48)
+GOLDEN = {1: 2, 2: 12, 3: 184, 4: 8512, 5: 1262816, 6: 575780564, 7: 789360053252,
+          8: 3266598486981642, 9: 41044208702632496804}  # scripts/test/golden_cpu.py:9-19
+
+# Residues published by the reference for its GPU solvers.
+KNOWN = [
+    (9, 4294967291, 2674633373), (9, 4294966997, 3332982389),    # scripts/test/groupbatch-runtime.py:17
+    (18, 4294967291, 503411004),                                 # docs/results/reverse-algorithm-2026-09-05.md:53
+    (16, 2147483647, 1234504449), (17, 2147483647, 1667553532),  # docs/b300-hbm32.md:479-481
+    (18, 2147483647, 624312750),
+    (20, 4294967291, 2308006916), (20, 4294966997, 3704549185),  # scripts/test/groupbatch-scratch.py:17
+    (21, 4294966997, 2124618149), (21, 4294967291, 998035516),   # scripts/run/autotune.py:28, docs/b300-hbm32.md:554
+]
+
+
+@pytest.mark.parametrize("n", list(range(1, 12)))
+def test_residues_match_oracle_plain_and_batched(engine, n):
+    mods = [P[0], P[10], 2, 3]
+    want = [orc.residue(n, m) for m in mods]
+    assert engine.residues(n, mods, lanes=1).residues == want
+    assert engine.residues(n, mods, lanes=4).residues == want
+
+
+def test_exact_counts_by_crt(engine):
+    for n, exact in GOLDEN.items():
+        mods = P[:3]
+        res = engine.residues(n, mods, lanes=3).residues
+        x, m = orc.crt(dict(zip(mods, res)))
+        assert m > exact and x == exact, n
+
+
+@pytest.mark.parametrize("n,mod,want", KNOWN)
+def test_published_residues(engine, n, mod, want):
+    assert engine.residues(n, [mod], lanes=1).residues == [want]
+
+
+def test_lane_counts_agree(engine):
+    n = 13
+    mods = P[:16]
+    plain = engine.residues(n, mods, lanes=1).residues
+    for lanes in (2, 5, 7, 16):
+        assert engine.residues(n, mods, lanes=lanes).residues == plain
+    assert plain[0] == orc.residue(n, mods[0])

@@ -12,7 +12,8 @@ value    residues/hour from the device time of the captured pass (CUDA events
 e2e      residues/hour through the public C ABI call fdp_run_sync from host
          buffers (moduli in, residues out) including graph capture.
 roofline the per-cell transition kernel: algorithmic bytes per launch
-         (4(M+D) + 4(Wm(p)+D) per modulus) over its CUDA-event duration.
+         (fdp_cell_bytes: 4 x words that must be read + 4 x words that can
+         change, per modulus) over its CUDA-event duration.
 
 --impl reference times the reference's own CPU counter (third_party/ggcount,
 built unmodified into oracle/_ref) on a bounded sample and scales it to the
@@ -318,6 +319,19 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def run_cells_only(args) -> None:
+    """One row sweep (cells p = n..1, one launch each) of lanes moduli on the
+    engine's resident state; prints the per-cell CUDA-event times."""
+    import fdp
+    lanes = args.lanes or min(args.k, fdp.MAX_LANES)
+    moduli = primes_below_2_32(lanes)
+    W = args.n + 1
+    with fdp.Engine(0) as eng:
+        ms = eng.time_cells(args.n, moduli, lanes, rows=args.profile_rows)
+    gbs = [fdp.cell_bytes(W, p) * lanes / (ms[p] * 1e-3) / 1e9 for p in range(1, W)]
+    print(json.dumps({"n": args.n, "lanes": lanes, "cell_ms": ms[1:], "cell_gbs": gbs}), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -330,8 +344,12 @@ def main() -> None:
     ap.add_argument("--profile-rows", type=int, default=1)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cells-only", action="store_true",
+                    help="profiling case: one row sweep of separately launched cells on a resident state")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.cells_only:
+        run_cells_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -71,7 +71,7 @@ typedef struct fdp_plan_out {
   uint64_t total_bytes;
   int rows;                         /* row sweeps per residue                     */
   int cells_per_row;                /* W - 1                                      */
-  uint64_t alg_bytes_per_residue;   /* sum over cells of 4(M+D) + 4(Wm(p)+D)      */
+  uint64_t alg_bytes_per_residue;   /* sum over cells of fdp_cell_bytes            */
   uint64_t transitions_per_residue; /* sum over cells of (M + D)                  */
   int fits;                         /* total_bytes <= budget                      */
 } fdp_plan_out;
@@ -145,7 +145,12 @@ fdp_status fdp_unrank_words(fdp_ctx *ctx, int width, const uint64_t *d_ranks, ui
 /* Ternary rank index on the device (src/common/ternary_rank_index.hpp:6-15). */
 fdp_status fdp_ternary_index(fdp_ctx *ctx, const uint32_t *d_codes, uint32_t *d_index, uint64_t count, void *stream);
 
-/* Host helpers: state counts and the per-cell algorithmic byte model. */
+/*
+ * Host helpers: state counts and the per-cell algorithmic byte model, the
+ * minimum traffic of one cell of the in-place sweep for one modulus:
+ * 4 x (every main word + the blocked input unless p = width-1)
+ * + 4 x (main words that can change + the blocked output unless p = 1).
+ */
 uint64_t fdp_main_states(int width);
 uint64_t fdp_blocked_states(int width);
 uint64_t fdp_cell_bytes(int width, int p);

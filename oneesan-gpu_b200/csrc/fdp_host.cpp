@@ -197,17 +197,26 @@ static void prefix_counts(int len, uint64_t *P /* FDP_HT */) {
 }
 
 uint64_t cell_bytes(int W, int p) {
+  // Minimum traffic of one cell of the in-place sweep, one modulus:
+  //   reads : every main word (identity words are closure sources), and the
+  //           blocked input except at p = W-1, where it is known to be zero;
+  //   writes: main words whose value can change (pair LR/NR/NL or N at p;
+  //           at p = 1 the pairs NN, LR, NR, RN) and the blocked output
+  //           except at p = 1, which produces none.
   const CountTable &c = counts();
   uint64_t M = main_states(W), D = blocked_states(W), wm = 0;
-  if (p == 1) {
-    wm = M;
-  } else {
-    uint64_t P[FDP_HT];
-    prefix_counts(W - 1 - p, P);
-    for (int h = 0; h < FDP_HT; ++h)
-      if (P[h]) wm += P[h] * (c.at(p, h) + c.at(p - 1, h));
+  uint64_t P[FDP_HT];
+  prefix_counts(W - 1 - p, P);
+  for (int h = 0; h < FDP_HT; ++h) {
+    if (!P[h]) continue;
+    if (p == 1)  // NN, LR (h = 0) and NR, RN (h = 1): one word each
+      wm += P[h] * ((h == 0 ? 2 : 0) + (h == 1 ? 2 : 0));
+    else
+      wm += P[h] * (c.at(p, h) + c.at(p - 1, h));
   }
-  return 4 * (M + D) + 4 * (wm + D);
+  const uint64_t rd = M + (p < W - 1 ? D : 0);
+  const uint64_t wr = wm + (p >= 2 ? D : 0);
+  return 4 * (rd + wr);
 }
 
 uint64_t row_bytes(int W) {

@@ -35,8 +35,9 @@ uint64_t first_row_state(uint64_t mask, int W);
 // include_horizontal (TR.hpp:113-144): 0 invalid, 1 main, 2 blocked.
 int include_horizontal(uint64_t m, int width, int p, uint64_t *out);
 
-// Algorithmic bytes of one cell p for one modulus:
-//   4(M+D) + 4(Wm(p)+D), Wm(p) = main targets that can change (p=1: all).
+// Algorithmic bytes of one cell p for one modulus: the minimum traffic of the
+// in-place sweep (the 4(M+D) + 4(Wm(p)+D) model without the blocked read at
+// p = W-1, which is known zero, and without the blocked write at p = 1).
 uint64_t cell_bytes(int W, int p);
 // Algorithmic bytes of one full row sweep p = W-1..1, one modulus.
 uint64_t row_bytes(int W);

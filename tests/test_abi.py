@@ -1,0 +1,85 @@
+"""C ABI: the library loads, exports every declared entry point, and the pure
+host planner returns the state sizes and byte model of the path.  CPU only."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import fdp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for f in os.listdir(inc):
+        if f.endswith(".h"):
+            text = open(os.path.join(inc, f)).read()
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            names |= set(re.findall(r"\b(fdp_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_exported():
+    lib = fdp.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 14
+    for s in syms:
+        assert hasattr(lib, s), s
+
+
+def test_version():
+    assert b"sm_100a" in fdp.lib().fdp_version()
+
+
+@pytest.mark.parametrize("n,M,D", [
+    (18, 32652735, 11662902), (20, 258215664, 91695540), (22, 2062967382, 728997192),
+    (23, 5850674704, 2062967382)])
+def test_state_counts(n, M, D):
+    # H_DP[W][1] / H_DP[W-1][1] as printed by the reference's PLAN_ONLY mode
+    assert fdp.main_states(n + 1) == M and fdp.blocked_states(n + 1) == D
+    pl = fdp.plan(n, [4294967291])
+    assert pl.main_states == M and pl.blocked_states == D
+    assert pl.state_bytes == 4 * (M + D) and pl.scratch_bytes == 0
+
+
+def test_plan_n22_batched():
+    pl = fdp.plan(22, list(range(4294967000, 4294967014)), lanes=14, budget=180 * 10**9)
+    assert pl.lanes == 14 and pl.passes == 1 and pl.fits == 1
+    assert abs(pl.state_bytes / 2**30 - 145.61) < 0.01
+    assert pl.rows == 21 and pl.cells_per_row == 22 and pl.index_bits == 32
+    assert fdp.plan(23, [7], lanes=1).index_bits == 64
+    # 16 lanes at n=23 need 471.7 GiB: does not fit a B200
+    assert fdp.plan(23, list(range(100, 116)), lanes=16, budget=180 * 10**9).fits == 0
+
+
+def test_byte_model():
+    W = 23
+    row = sum(fdp.cell_bytes(W, p) for p in range(1, W))
+    assert abs(row / 1e9 - 392.77) < 0.01
+    M, D = fdp.main_states(W), fdp.blocked_states(W)
+    # p = W-1: no blocked read; p = 1: no blocked write
+    assert fdp.cell_bytes(W, W - 1) < 4 * (M + D) + 4 * (M + D)
+    assert fdp.cell_bytes(W, 0) == 0 and fdp.cell_bytes(W, W) == 0
+
+
+def test_plan_rejects_bad_problems():
+    with pytest.raises(fdp.FdpError) as e:
+        fdp.plan(0, [7])
+    assert e.value.status == fdp.FDP_ERR_ARGS
+    with pytest.raises(fdp.FdpError) as e:
+        fdp.plan(10, [1])
+    assert e.value.status == fdp.FDP_ERR_MODULUS
+    with pytest.raises(fdp.FdpError):
+        fdp.plan(10, [7], lanes=17)
+
+
+def test_create_without_gpu_reports_gpu_count():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    with pytest.raises(fdp.FdpError) as e:
+        fdp.Engine(0)
+    assert e.value.status == fdp.FDP_ERR_GPU_COUNT

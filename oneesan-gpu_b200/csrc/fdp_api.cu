@@ -312,3 +312,7 @@ extern "C" fdp_status fdp_time_cells(fdp_ctx *c, const fdp_problem *pr, int rows
   for (auto &e : ev) cudaEventDestroy(e);
   return rs;
 }
+
+// Lets other translation units of the library report a message through
+// fdp_last_error().
+void fdp_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }

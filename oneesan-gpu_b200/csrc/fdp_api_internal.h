@@ -28,3 +28,4 @@ fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const fdp::DevTables **out);
 fdp_status fdp_enqueue_pass(fdp_ctx *c, const fdp::DevTables &t, int L, const uint32_t *mods, uint32_t *main,
                             uint32_t *blk, unsigned long long *acc, uint32_t *d_res, uint32_t *h_res,
                             cudaStream_t s, uint64_t *launches);
+void fdp_set_last_error(const char *msg);

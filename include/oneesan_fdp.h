@@ -20,8 +20,13 @@
  *   - One context per device; calls on one context are serialised by the
  *     caller, except fdp_submit / fdp_poll, which are thread-safe.
  *   - Residues are canonical in [0, p); moduli are in [2, 2^32 - 1].
- *   - Coefficient vectors are in canonical rank order (GB.cu:1568 rank_full)
- *     with `lanes` residues interleaved per state: word[state * lanes + l].
+ *   - Coefficient vectors are in canonical rank order (GB.cu:1568 rank_full).
+ *     The `lanes` residues of a state (one per modulus) are stored in panels:
+ *     lanes are grouped greedily 8, 4, 2, 1 at a time (lanes = 14 -> panels
+ *     {0-7}, {8-11}, {12-13}); the panel whose first lane is L0 and whose
+ *     width is PW is an array [N][PW] that starts at word L0 * N, where N is
+ *     the number of states of the vector.  For lanes = 1, 2, 4 or 8 this is
+ *     the plain interleaved layout word[state * lanes + l].
  */
 #ifndef ONEESAN_FDP_H
 #define ONEESAN_FDP_H
@@ -111,7 +116,8 @@ fdp_status fdp_run_sync(fdp_ctx *ctx, const fdp_problem *problem, uint32_t *resi
 
 /*
  * Operator level: apply cells p_hi, p_hi-1, ..., p_lo of one row sweep to
- * caller-owned device vectors (width = n+1, main [M][lanes], block [D][lanes]).
+ * caller-owned device vectors (width = n+1, main: lanes x M words, block:
+ * lanes x D words, both in the panel layout above).
  * The blocked input is consumed at p_hi; the blocked output of p_lo is left in
  * `block` (all zero when p_lo = 1).  Replaces process_window_batched_io for a
  * window (GB.cu:1701-1742) as exercised by tests/groupbatch_operator_test.cu,
@@ -135,6 +141,23 @@ fdp_status fdp_apply_cells(fdp_ctx *ctx, int width, int p_hi, int p_lo, int lane
  * timers of GRIDFP_PROFILE_BATCH=1 (src/cuda/b300/factor_transfer_batch.cuh:110-158).
  */
 fdp_status fdp_time_cells(fdp_ctx *ctx, const fdp_problem *problem, int rows, double *cell_ms);
+
+/*
+ * Launch tuning of the cell kernel for this context (what the autotuner sets;
+ * the reference's GRIDFP_THREADS and scheduling knobs, GB.cu:2190,
+ * scripts/run/autotune.py:157-300).  block: threads per CTA (64..256, a
+ * multiple of 32); grid: CTAs per launch (0 = sized from occupancy, a multiple
+ * of the SM count); split_panels: for lane counts that need several panels,
+ * run one launch per panel instead of one launch that stages closure sources
+ * in shared memory.  Results never depend on these settings.
+ */
+typedef struct fdp_tuning {
+  int block;
+  int grid;
+  int split_panels;
+} fdp_tuning;
+fdp_status fdp_set_tuning(fdp_ctx *ctx, const fdp_tuning *tuning);
+fdp_status fdp_get_tuning(fdp_ctx *ctx, fdp_tuning *tuning);
 
 /* Canonical rank / unrank of frontier words on the device (GB.cu:1568 rank_full). */
 fdp_status fdp_rank_words(fdp_ctx *ctx, int width, const uint64_t *d_words, uint64_t *d_ranks, uint64_t count,

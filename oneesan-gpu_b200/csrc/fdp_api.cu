@@ -316,3 +316,25 @@ extern "C" fdp_status fdp_time_cells(fdp_ctx *c, const fdp_problem *pr, int rows
 // Lets other translation units of the library report a message through
 // fdp_last_error().
 void fdp_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
+extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
+  if (!c || !t) return FDP_ERR_ARGS;
+  if (t->block < 64 || t->block > 256 || t->block % 32 || t->grid < 0) {
+    g_last_error = "tuning: block must be a multiple of 32 in 64..256 and grid >= 0";
+    return FDP_ERR_ARGS;
+  }
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->cfg.block = t->block;
+  c->cfg.grid = t->grid;
+  c->cfg.split_panels = t->split_panels != 0;
+  return FDP_OK;
+}
+
+extern "C" fdp_status fdp_get_tuning(fdp_ctx *c, fdp_tuning *t) {
+  if (!c || !t) return FDP_ERR_ARGS;
+  std::lock_guard<std::mutex> lk(c->mu);
+  t->block = c->cfg.block;
+  t->grid = c->cfg.grid;
+  t->split_panels = c->cfg.split_panels ? 1 : 0;
+  return FDP_OK;
+}

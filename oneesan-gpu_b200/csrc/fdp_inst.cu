@@ -15,19 +15,22 @@ namespace fdp {
 
 template <typename Idx, int K>
 cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t s) {
-  int grid = cfg.grid;
-  if (grid <= 0) {
-    static int per_sm = 0;  // resident CTAs per SM for this variant
-    if (!per_sm) {
-      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cell_kernel<Idx, K>, cfg.block, 0);
-      if (e != cudaSuccess) return e;
-      if (per_sm < 1) per_sm = 1;
-    }
-    grid = device_sm_count() * per_sm;
+  const size_t smem = cell_smem_bytes<Idx, K>(cfg.block);
+  // Per-variant state, resolved on first use (the device is the same for the
+  // life of the process in this library's contexts).
+  static int configured_block = 0, per_sm = 0;
+  if (configured_block != cfg.block) {
+    cudaError_t e = cudaFuncSetAttribute(cell_kernel<Idx, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cell_kernel<Idx, K>, cfg.block, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    configured_block = cfg.block;
   }
+  int grid = cfg.grid > 0 ? cfg.grid : device_sm_count() * per_sm;
   const uint64_t need = (a.items + cfg.block - 1) / cfg.block;
   if (uint64_t(grid) > need) grid = int(need ? need : 1);
-  cell_kernel<Idx, K><<<grid, cfg.block, 0, s>>>(a);
+  cell_kernel<Idx, K><<<grid, cfg.block, smem, s>>>(a);
   return cudaGetLastError();
 }
 

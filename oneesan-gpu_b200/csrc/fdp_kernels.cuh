@@ -12,24 +12,34 @@ namespace fdp {
 template <typename Idx>
 __device__ __forceinline__ void load_cell_smem(CellSmem<Idx> &sm, const WidthTables<Idx> *t, int W, int p) {
   const int nthr = blockDim.x, tid = threadIdx.x;
-  for (int i = tid; i < (FDP_MAXW + 1) * FDP_HT; i += nthr) (&sm.H[0][0])[i] = (&t->H[0][0])[i];
+  for (int i = tid; i < (FDP_MAXW + 1) * FDP_HS; i += nthr) sm.H[i / FDP_HS][i % FDP_HS] = t->H[i / FDP_HS][i % FDP_HS];
   // Only blocked positions p..W-2 are walked by the prefix decode.
   const int rows = W - 1 - p;
-  for (int i = tid; i < rows * FDP_HT; i += nthr) {
-    const int pos = p + i / FDP_HT, h = i % FDP_HT;
+  for (int i = tid; i < rows * FDP_HS; i += nthr) {
+    const int pos = p + i / FDP_HS, h = i % FDP_HS;
     sm.S[pos][h] = t->S[pos][h];
   }
-  for (int i = tid; i < FDP_HT * PR_COUNT; i += nthr) (&sm.OFF[0][0])[i] = (&t->OFF[p][0][0])[i];
+  for (int i = tid; i < FDP_HS * PR_COUNT; i += nthr) sm.OFF[i / PR_COUNT][i % PR_COUNT] = t->OFF[p][i / PR_COUNT][i % PR_COUNT];
+}
+
+// Dynamic shared memory of the cell kernel: the width tables, then the
+// closure-candidate slots (slot i of thread t at cand[i * blockDim + t]).
+template <typename Idx, int K>
+constexpr size_t cell_smem_bytes(int block) {
+  return sizeof(CellSmem<Idx>) + (stages_candidates<K>() ? size_t(FDP_MAX_CAND) * block * sizeof(Idx) : 0);
 }
 
 template <typename Idx, int K>
 __global__ void __launch_bounds__(256) cell_kernel(const CellArgs a) {
-  __shared__ CellSmem<Idx> sm;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CellSmem<Idx> &sm = *reinterpret_cast<CellSmem<Idx> *>(smem_raw);
+  Idx *cand = reinterpret_cast<Idx *>(smem_raw + sizeof(CellSmem<Idx>));
   load_cell_smem<Idx>(sm, reinterpret_cast<const WidthTables<Idx> *>(a.tables), a.W, a.p);
   __syncthreads();
   const Idx n = Idx(a.items);
   const Idx stride = Idx(gridDim.x) * blockDim.x;
-  for (Idx j = Idx(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride) cell_item<Idx, K>(a, sm, j);
+  for (Idx j = Idx(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride)
+    cell_item<Idx, K>(a, sm, j, cand + threadIdx.x, int(blockDim.x));
 }
 
 template <typename Idx, int K>
@@ -45,7 +55,7 @@ __global__ void __launch_bounds__(256) first_row_init_kernel(const FirstRowArgs 
   for (uint64_t mask = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; mask < total;
        mask += uint64_t(gridDim.x) * blockDim.x) {
     const Idx rk = rank_dev<Idx>(first_row_state_dev(mask, a.W), a.W, sH);
-    stk<K>(a.main + size_t(rk) * K, one);
+    st_lanes<K>(a.main, a.mstates, size_t(rk), one);
   }
 }
 
@@ -64,7 +74,7 @@ __global__ void __launch_bounds__(256) first_row_dot_kernel(const FirstRowArgs a
        mask += uint64_t(gridDim.x) * blockDim.x) {
     const Idx rk = rank_dev<Idx>(first_row_state_dev(mask, a.W), a.W, sH);
     uint32_t v[K];
-    ldk<K>(a.main + size_t(rk) * K, v);
+    ld_lanes<K>(a.main, a.mstates, size_t(rk), v);
 #pragma unroll
     for (int i = 0; i < K; ++i) acc[i] += v[i];
   }

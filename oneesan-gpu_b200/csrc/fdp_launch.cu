@@ -56,19 +56,7 @@ void free_tables(DevTables *t) {
     default: return cudaErrorInvalidValue; \
   }
 
-cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_t *main, uint32_t *blk, int p,
-                        bool blk_in_zero, bool blk_out_p1, const LaunchCfg &cfg, cudaStream_t s) {
-  if (!t.ptr || p < 1 || p >= t.W || K < 1 || K > kMaxLanes) return cudaErrorInvalidValue;
-  CellArgs a{};
-  a.tables = t.ptr;
-  a.main = main;
-  a.blk = blk;
-  a.items = blocked_states(t.W);
-  for (int i = 0; i < K; ++i) a.mod[i] = mods[i];
-  a.W = t.W;
-  a.p = p;
-  a.blk_in_zero = blk_in_zero ? 1 : 0;
-  a.blk_out_p1 = blk_out_p1 ? 1 : 0;
+static cudaError_t launch_cell_k(const DevTables &t, int K, const CellArgs &a, const LaunchCfg &cfg, cudaStream_t s) {
   if (t.u64) {
 #define CALL64(k) launch_cell_t<uint64_t, k>(a, cfg, s)
     FDP_SWITCH_K(K, CALL64)
@@ -79,6 +67,36 @@ cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_
 #undef CALL32
 }
 
+cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_t *main, uint32_t *blk, int p,
+                        bool blk_in_zero, bool blk_out_p1, const LaunchCfg &cfg, cudaStream_t s) {
+  if (!t.ptr || p < 1 || p >= t.W || K < 1 || K > kMaxLanes) return cudaErrorInvalidValue;
+  CellArgs a{};
+  a.tables = t.ptr;
+  a.main = main;
+  a.blk = blk;
+  a.items = blocked_states(t.W);
+  a.mstates = main_states(t.W);
+  for (int i = 0; i < K; ++i) a.mod[i] = mods[i];
+  a.W = t.W;
+  a.p = p;
+  a.blk_in_zero = blk_in_zero ? 1 : 0;
+  a.blk_out_p1 = blk_out_p1 ? 1 : 0;
+  const bool one_panel = (K == 1 || K == 2 || K == 4 || K == 8);
+  if (one_panel || !cfg.split_panels) return launch_cell_k(t, K, a, cfg, s);
+  // Every panel is an independent [N][PW] array: run each as its own K = PW problem.
+  for (int l0 = 0; l0 < K;) {
+    const int pw = (K - l0 >= 8) ? 8 : (K - l0 >= 4) ? 4 : (K - l0 >= 2) ? 2 : 1;
+    CellArgs b = a;
+    b.main = main + size_t(l0) * a.mstates;
+    b.blk = blk + size_t(l0) * a.items;
+    for (int i = 0; i < pw; ++i) b.mod[i] = mods[l0 + i];
+    cudaError_t e = launch_cell_k(t, pw, b, cfg, s);
+    if (e != cudaSuccess) return e;
+    l0 += pw;
+  }
+  return cudaSuccess;
+}
+
 static cudaError_t first_row(const DevTables &t, int K, const uint32_t *mods, uint32_t *main,
                              unsigned long long *acc, bool dot, cudaStream_t s) {
   if (!t.ptr || K < 1 || K > kMaxLanes) return cudaErrorInvalidValue;
@@ -86,6 +104,7 @@ static cudaError_t first_row(const DevTables &t, int K, const uint32_t *mods, ui
   a.tables = t.ptr;
   a.main = main;
   a.acc = acc;
+  a.mstates = main_states(t.W);
   for (int i = 0; i < K && mods; ++i) a.mod[i] = mods[i];
   a.W = t.W;
   if (t.u64) {

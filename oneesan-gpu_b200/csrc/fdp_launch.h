@@ -21,7 +21,8 @@ void free_tables(DevTables *t);
 
 struct LaunchCfg {
   int block = 256;
-  int grid = 0;  // 0: sized from occupancy (a multiple of the SM count)
+  int grid = 0;              // 0: sized from occupancy (a multiple of the SM count)
+  bool split_panels = false; // several panels: one single-panel launch per panel
 };
 
 template <typename Idx, int K>

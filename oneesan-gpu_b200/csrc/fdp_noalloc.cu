@@ -58,7 +58,7 @@ struct Mods {
 
 template <int K>
 __global__ void __launch_bounds__(256) noalloc_dot_kernel(const ull *__restrict__ counts, const uint32_t *main,
-                                                          ull *acc_out, int W) {
+                                                          uint64_t mstates, ull *acc_out, int W) {
   __shared__ ull sH[FDP_MAXW + 1][FDP_HT];
   __shared__ ull red[8][K];
   for (int i = threadIdx.x; i < (FDP_MAXW + 1) * FDP_HT; i += blockDim.x) (&sH[0][0])[i] = counts[i];
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) noalloc_dot_kernel(const ull *__restrict_
        mask += uint64_t(gridDim.x) * blockDim.x) {
     const ull rk = fdp::rank_dev<ull>(fdp::first_row_state_dev(mask, W), W, sH);
     uint32_t v[K];
-    fdp::ldk<K>(main + size_t(rk) * K, v);
+    fdp::ld_lanes<K>(main, mstates, size_t(rk), v);
 #pragma unroll
     for (int i = 0; i < K; ++i) acc[i] += v[i];
   }
@@ -99,7 +99,7 @@ cudaError_t launch_dot(const DeviceSetup &s, const uint32_t *main, int W, cudaSt
   const uint64_t total = 1ull << (W - 1);
   uint64_t blocks = (total + 255) / 256;
   if (blocks > 1184) blocks = 1184;
-  noalloc_dot_kernel<K><<<unsigned(blocks), 256, 0, st>>>(s.counts, main, s.acc, W);
+  noalloc_dot_kernel<K><<<unsigned(blocks), 256, 0, st>>>(s.counts, main, fdp::main_states(W), s.acc, W);
   return cudaGetLastError();
 }
 

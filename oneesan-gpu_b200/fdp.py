@@ -50,6 +50,10 @@ class PlanOut(ctypes.Structure):
                 ("transitions_per_residue", ctypes.c_uint64), ("fits", ctypes.c_int)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int), ("grid", ctypes.c_int), ("split_panels", ctypes.c_int)]
+
+
 class RunStats(ctypes.Structure):
     _fields_ = [("wall_s", ctypes.c_double), ("device_s", ctypes.c_double),
                 ("capture_s", ctypes.c_double), ("kernel_launches", ctypes.c_uint64),
@@ -78,6 +82,8 @@ def lib() -> ctypes.CDLL:
     L.fdp_run_sync.argtypes = [c_vp, P(Problem), P(c_u32), P(RunStats)]
     L.fdp_apply_cells.argtypes = [c_vp, c_int, c_int, c_int, c_int, P(c_u32), c_vp, c_vp, c_vp]
     L.fdp_time_cells.argtypes = [c_vp, P(Problem), c_int, P(ctypes.c_double)]
+    L.fdp_set_tuning.argtypes = [c_vp, P(Tuning)]
+    L.fdp_get_tuning.argtypes = [c_vp, P(Tuning)]
     L.fdp_rank_words.argtypes = [c_vp, c_int, c_vp, c_vp, c_u64, c_vp]
     L.fdp_unrank_words.argtypes = [c_vp, c_int, c_vp, c_vp, c_u64, c_vp]
     L.fdp_ternary_index.argtypes = [c_vp, c_vp, c_vp, c_u64, c_vp]
@@ -98,6 +104,37 @@ def _check(status: int, where: str) -> None:
 
 def _u32_array(values: Sequence[int]):
     return (ctypes.c_uint32 * len(values))(*[int(v) for v in values])
+
+
+def lane_panels(lanes: int) -> list:
+    """Panels (first lane, width) of the lane layout: greedy widths 8, 4, 2, 1."""
+    out, l0 = [], 0
+    while l0 < lanes:
+        pw = 8 if lanes - l0 >= 8 else 4 if lanes - l0 >= 4 else (2 if lanes - l0 >= 2 else 1)
+        out.append((l0, pw))
+        l0 += pw
+    return out
+
+
+def pack_lanes(a):
+    """(N, lanes) uint32 array -> flat array in the engine's panel layout."""
+    import numpy as np
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    n, lanes = a.shape
+    out = np.empty(n * lanes, dtype=np.uint32)
+    for l0, pw in lane_panels(lanes):
+        out[l0 * n:(l0 + pw) * n] = a[:, l0:l0 + pw].reshape(-1)
+    return out
+
+
+def unpack_lanes(flat, n: int, lanes: int):
+    """Inverse of pack_lanes."""
+    import numpy as np
+    flat = np.asarray(flat, dtype=np.uint32).reshape(-1)
+    out = np.empty((n, lanes), dtype=np.uint32)
+    for l0, pw in lane_panels(lanes):
+        out[:, l0:l0 + pw] = flat[l0 * n:(l0 + pw) * n].reshape(n, pw)
+    return out
 
 
 def main_states(width: int) -> int:
@@ -166,6 +203,15 @@ class Engine:
         out = (ctypes.c_double * (n + 1))()
         _check(lib().fdp_time_cells(self._ctx, ctypes.byref(pr), rows, out), "fdp_time_cells")
         return [float(x) for x in out]
+
+    def set_tuning(self, block: int = 256, grid: int = 0, split_panels: bool = False) -> None:
+        t = Tuning(block, grid, 1 if split_panels else 0)
+        _check(lib().fdp_set_tuning(self._ctx, ctypes.byref(t)), "fdp_set_tuning")
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        _check(lib().fdp_get_tuning(self._ctx, ctypes.byref(t)), "fdp_get_tuning")
+        return {"block": t.block, "grid": t.grid, "split_panels": bool(t.split_panels)}
 
     def apply_cells(self, width: int, p_hi: int, p_lo: int, moduli: Sequence[int], main_ptr: int,
                     block_ptr: int, stream: int = 0) -> None:

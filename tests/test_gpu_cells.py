@@ -25,11 +25,13 @@ def _rand(rng, n, lanes, mods):
 
 def _device(a):
     import torch
-    return torch.from_numpy(a.view(np.int32).copy()).cuda()
+    import fdp
+    return torch.from_numpy(fdp.pack_lanes(a).view(np.int32)).cuda()
 
 
-def _host(t):
-    return t.cpu().numpy().view(np.uint32)
+def _host(t, n, lanes):
+    import fdp
+    return fdp.unpack_lanes(t.cpu().numpy().view(np.uint32), n, lanes)
 
 
 def _oracle_window(width, p_hi, p_lo, mods, main, block):
@@ -54,7 +56,7 @@ def _run(engine, width, p_hi, p_lo, mods, seed, replays=1):
         dm, db = _device(main), _device(block)
         engine.apply_cells(width, p_hi, p_lo, mods, dm.data_ptr(), db.data_ptr())
         torch.cuda.synchronize()
-        got_m, got_b = _host(dm).reshape(M, len(mods)), _host(db).reshape(D, len(mods))
+        got_m, got_b = _host(dm, M, len(mods)), _host(db, D, len(mods))
         np.testing.assert_array_equal(got_m, want_m)
         np.testing.assert_array_equal(got_b, want_b)
 
@@ -90,3 +92,22 @@ def test_zero_input_stays_zero(engine):
     engine.apply_cells(width, width - 1, 1, [4294967291, 2], dm.data_ptr(), db.data_ptr())
     torch.cuda.synchronize()
     assert int(dm.abs().sum()) == 0 and int(db.abs().sum()) == 0
+
+
+def test_tuning_never_changes_results(engine):
+    # block size, grid size and panel splitting are performance knobs only
+    try:
+        for block, grid, split in ((128, 0, True), (64, 37, False), (256, 1, True), (96, 0, False)):
+            engine.set_tuning(block=block, grid=grid, split_panels=split)
+            assert engine.get_tuning() == {"block": block, "grid": grid, "split_panels": split}
+            _run(engine, 12, 11, 1, [MODS[i % 3] for i in range(14)], seed=block + grid)
+    finally:
+        engine.set_tuning()
+
+
+def test_tuning_rejects_bad_block(engine):
+    import fdp
+    with pytest.raises(fdp.FdpError):
+        engine.set_tuning(block=100)
+    with pytest.raises(fdp.FdpError):
+        engine.set_tuning(block=512)

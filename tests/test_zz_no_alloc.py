@@ -42,7 +42,7 @@ def test_noalloc_matches_run_sync_on_two_calls(engine):
     init = np.zeros((M, lanes), dtype=np.uint32)
     for mask in range(1 << (W - 1)):
         init[orc.rank(int(orc.lib().oracle_first_row_state(mask, W)), W), :] = 1
-    dm = torch.from_numpy(init.reshape(-1).view(np.int32).copy()).cuda()
+    dm = torch.from_numpy(fdp.pack_lanes(init).view(np.int32)).cuda()
     db = torch.zeros(D * lanes, dtype=torch.int32, device="cuda")
     for _row in range(1, W - 1):
         engine.apply_cells(W, W - 1, 1, moduli, dm.data_ptr(), db.data_ptr())

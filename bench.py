@@ -319,6 +319,70 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def run_serving(args) -> None:
+    """The serving stream: seeded Poisson arrivals, n ~ U{12..21}, k ~ U{1..8}
+    largest-below-2^32 primes, admission under an HBM budget."""
+    import random
+    import threading as th
+    import fdp
+    rng = random.Random(args.seed)
+    primes = primes_below_2_32(8)
+    reqs, t = [], 0.0
+    for _ in range(args.serve_requests):
+        t += rng.expovariate(1.0 / args.serve_gap)
+        n = rng.randint(12, 21)
+        k = rng.randint(1, 8)
+        reqs.append((t * args.serve_time_scale, n, primes[:k]))
+    eng = fdp.Engine(0)
+    # warm-up: tables and kernels for every n of the stream
+    for n in sorted({r[1] for r in reqs}):
+        eng.residues(n, primes[:1], 1)
+    eng.server_start(int(args.serve_budget_gb * 1e9), max_active=args.serve_slots, max_lanes=8)
+    ids = [None] * len(reqs)
+    t0 = time.perf_counter()
+    def submitter():
+        for i, (at, n, mods) in enumerate(reqs):
+            d = at - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            ids[i] = eng.submit(n, mods)
+    sub = th.Thread(target=submitter)
+    sub.start()
+    sampler = ClockSampler(0)
+    sampler.start()
+    results = []
+    for i in range(len(reqs)):
+        while ids[i] is None:
+            time.sleep(0.001)
+        r = eng.wait(ids[i], timeout_ms=3600 * 1000)
+        results.append(r)
+    makespan = time.perf_counter() - t0
+    sub.join()
+    clocks = sampler.stop()
+    stats = eng.server_stats()
+    eng.server_stop()
+    lat = sorted(r["latency_s"] for r in results)
+    def pct(q):
+        return lat[min(len(lat) - 1, int(q * len(lat)))]
+    residues = sum(len(m) for _, _, m in reqs)
+    line = {
+        "metric": "serving stream latency and throughput (continuous batching)", "value": pct(0.5),
+        "unit": "s (p50 latency)", "higher_is_better": False, "n_gpus": 1, "dtype": "u32",
+        "config": {"workload": f"seed {args.seed}: {len(reqs)} requests, Poisson arrivals mean gap "
+                               f"{args.serve_gap} s x time scale {args.serve_time_scale}, n~U{{12..21}}, "
+                               f"k~U{{1..8}} largest primes below 2^32", "budget_gb": args.serve_budget_gb,
+                   "slots": args.serve_slots, "max_lanes": 8},
+        "p50_latency_s": pct(0.5), "p99_latency_s": pct(0.99), "max_latency_s": lat[-1],
+        "mean_queue_s": statistics.mean(r["queue_s"] for r in results),
+        "throughput_residues_per_hour": 3600.0 * residues / makespan,
+        "throughput_requests_per_s": len(reqs) / makespan, "makespan_s": makespan,
+        "peak_running": stats["peak_running"], "peak_gb_in_use": stats["peak_bytes_in_use"] / 1e9,
+        "completed": stats["completed"], "failed": stats["failed"], "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def run_cells_only(args) -> None:
     """One row sweep (cells p = n..1, one launch each) of lanes moduli on the
     engine's resident state; prints the per-cell CUDA-event times."""
@@ -344,10 +408,19 @@ def main() -> None:
     ap.add_argument("--profile-rows", type=int, default=1)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve", action="store_true", help="run the serving stream instead")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-gap", type=float, default=2.0)
+    ap.add_argument("--serve-time-scale", type=float, default=1.0)
+    ap.add_argument("--serve-budget-gb", type=float, default=120.0)
+    ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--cells-only", action="store_true",
                     help="profiling case: one row sweep of separately launched cells on a resident state")
     args = ap.parse_args()
-    if args.cells_only:
+    if args.serve:
+        run_serving(args)
+    elif args.cells_only:
         run_cells_only(args)
     elif args.impl == "reference":
         run_reference(args)

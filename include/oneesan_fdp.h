@@ -115,6 +115,17 @@ void fdp_destroy(fdp_ctx *ctx);
 fdp_status fdp_run_sync(fdp_ctx *ctx, const fdp_problem *problem, uint32_t *residues_out, fdp_run_stats *stats);
 
 /*
+ * Several problems (grid sizes and moduli sets) in ONE captured CUDA graph:
+ * each problem's passes are captured on its own forked stream, joined at the
+ * end, and the graph runs with a single launch, so the problems overlap on the
+ * GPU.  residues_out receives the residues of problem 0, then problem 1, ...
+ * (sum of k entries).  stats covers the whole graph.  No counterpart in the
+ * reference, which runs one n per binary (SURVEY north star "batched" form).
+ */
+fdp_status fdp_run_multi_sync(fdp_ctx *ctx, const fdp_problem *problems, int count, uint32_t *residues_out,
+                              fdp_run_stats *stats);
+
+/*
  * Operator level: apply cells p_hi, p_hi-1, ..., p_lo of one row sweep to
  * caller-owned device vectors (width = n+1, main: lanes x M words, block:
  * lanes x D words, both in the panel layout above).
@@ -158,6 +169,56 @@ typedef struct fdp_tuning {
 } fdp_tuning;
 fdp_status fdp_set_tuning(fdp_ctx *ctx, const fdp_tuning *tuning);
 fdp_status fdp_get_tuning(fdp_ctx *ctx, fdp_tuning *tuning);
+
+/*
+ * Serving: a request loop with continuous batching.  No counterpart in the
+ * reference, which runs one process per job (SURVEY north star "served" form).
+ *
+ * fdp_server_start reserves hbm_budget_bytes of device memory once and starts
+ * a scheduler thread.  Requests (n, moduli) queue in arrival order; a request
+ * is admitted as soon as one of max_active slots and enough of the reserved
+ * pool are free (its frontier, 4 (M+D) lanes bytes, stays on the device until
+ * it finishes).  Later, smaller requests may pass a request that does not fit
+ * yet, unless it has waited longer than max_bypass_s.  Each admitted request
+ * runs its residue pass(es) as one CUDA graph on its own stream, so admitted
+ * requests overlap on the GPU and finish independently.  Results are exact and
+ * the same as fdp_run_sync's for the same problem.
+ */
+typedef struct fdp_server_config {
+  uint64_t hbm_budget_bytes;  /* device pool reserved for frontiers              */
+  int max_active;             /* concurrent requests on the GPU (1..64)          */
+  int max_lanes;              /* residues per pass of one request (1..16)        */
+  double max_bypass_s;        /* backfill limit; <= 0 means 30 s                  */
+} fdp_server_config;
+
+typedef struct fdp_request_info {
+  double queue_s;      /* submit -> admitted                                     */
+  double run_s;        /* admitted -> completion seen by the scheduler           */
+  double latency_s;    /* submit -> completion                                   */
+  double device_s;     /* CUDA-event time of the request's graph                 */
+  int lanes, passes;
+  uint64_t state_bytes;
+} fdp_request_info;
+
+typedef struct fdp_server_stats {
+  uint64_t submitted, completed, failed, queued, running;
+  uint64_t pool_bytes, bytes_in_use, peak_bytes_in_use;
+  int peak_running;
+} fdp_server_stats;
+
+fdp_status fdp_server_start(fdp_ctx *ctx, const fdp_server_config *config);
+/* Stops admitting, fails queued requests, waits for running ones, frees the pool. */
+fdp_status fdp_server_stop(fdp_ctx *ctx);
+/* Queue a request (problem->lanes is ignored; max_lanes applies).  Thread-safe.
+ * FDP_ERR_HBM if it can never fit the pool. */
+fdp_status fdp_submit(fdp_ctx *ctx, const fdp_problem *problem, uint64_t *request_id);
+/* FDP_PENDING while queued or running; FDP_OK copies k residues, fills info
+ * and forgets the request; an error status for a failed request.  Thread-safe. */
+fdp_status fdp_poll(fdp_ctx *ctx, uint64_t request_id, uint32_t *residues_out, fdp_request_info *info);
+/* fdp_poll with a bounded wait: FDP_TIMEOUT after timeout_ms. */
+fdp_status fdp_wait(fdp_ctx *ctx, uint64_t request_id, int timeout_ms, uint32_t *residues_out,
+                    fdp_request_info *info);
+fdp_status fdp_server_get_stats(fdp_ctx *ctx, fdp_server_stats *stats);
 
 /* Canonical rank / unrank of frontier words on the device (GB.cu:1568 rank_full). */
 fdp_status fdp_rank_words(fdp_ctx *ctx, int width, const uint64_t *d_words, uint64_t *d_ranks, uint64_t count,

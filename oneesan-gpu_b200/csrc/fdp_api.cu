@@ -113,6 +113,7 @@ extern "C" fdp_status fdp_create(fdp_ctx **out, int device) {
 }
 
 fdp_ctx::~fdp_ctx() {
+  fdp_server_shutdown(this);
   cudaSetDevice(device);
   if (stream) cudaStreamSynchronize(stream);
   for (auto &kv : tables) fdp::free_tables(&kv.second);
@@ -129,6 +130,7 @@ fdp_ctx::~fdp_ctx() {
 extern "C" void fdp_destroy(fdp_ctx *ctx) { delete ctx; }
 
 fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const DevTables **out) {
+  std::lock_guard<std::mutex> lk(c->tables_mu);
   auto it = c->tables.find(W);
   if (it == c->tables.end()) {
     DevTables t;
@@ -313,6 +315,8 @@ extern "C" fdp_status fdp_time_cells(fdp_ctx *c, const fdp_problem *pr, int rows
   return rs;
 }
 
+fdp_status fdp_cuda_status(cudaError_t e, const char *what) { return cuda_status(e, what); }
+
 // Lets other translation units of the library report a message through
 // fdp_last_error().
 void fdp_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
@@ -337,4 +341,114 @@ extern "C" fdp_status fdp_get_tuning(fdp_ctx *c, fdp_tuning *t) {
   t->grid = c->cfg.grid;
   t->split_panels = c->cfg.split_panels ? 1 : 0;
   return FDP_OK;
+}
+
+// One problem of fdp_run_multi_sync: its buffers and its forked stream.
+struct MultiPart {
+  const DevTables *t = nullptr;
+  int lanes = 1;
+  uint32_t *main = nullptr, *blk = nullptr, *res = nullptr;
+  unsigned long long *acc = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t done = nullptr;
+};
+
+extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, int count, uint32_t *residues_out,
+                                         fdp_run_stats *st) {
+  if (!c || !probs || count < 1 || count > 64 || !residues_out) return FDP_ERR_ARGS;
+  int total_k = 0;
+  for (int i = 0; i < count; ++i) {
+    fdp_status s = check_problem(&probs[i]);
+    if (s != FDP_OK) return s;
+    total_k += probs[i].k;
+  }
+  std::lock_guard<std::mutex> lk(c->mu);
+  auto t0 = std::chrono::steady_clock::now();
+  FDP_CK(cudaSetDevice(c->device), "cudaSetDevice");
+  std::vector<MultiPart> parts(static_cast<size_t>(count));
+  uint32_t *pinned = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  fdp_status rs = FDP_OK;
+  uint64_t launches = 0;
+  auto cleanup = [&]() {
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    for (size_t i = 0; i < parts.size(); ++i) {
+      MultiPart &p = parts[i];
+      if (p.main) cudaFree(p.main);
+      if (p.blk) cudaFree(p.blk);
+      if (p.acc) cudaFree(p.acc);
+      if (p.res) cudaFree(p.res);
+      if (p.s) cudaStreamDestroy(p.s);
+      if (p.done) cudaEventDestroy(p.done);
+    }
+    if (pinned) cudaFreeHost(pinned);
+    if (fork) cudaEventDestroy(fork);
+  };
+#define MULTI_CK(expr, what)                   \
+  do {                                         \
+    rs = cuda_status((expr), (what));          \
+    if (rs != FDP_OK) { cleanup(); return rs; } \
+  } while (0)
+  MULTI_CK(cudaMallocHost(&pinned, sizeof(uint32_t) * size_t(total_k)), "pinned residues");
+  MULTI_CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
+  for (int i = 0; i < count; ++i) {
+    MultiPart &p = parts[size_t(i)];
+    const int W = probs[i].n + 1;
+    if ((rs = fdp_ctx_tables(c, W, &p.t)) != FDP_OK) { cleanup(); return rs; }
+    p.lanes = probs[i].lanes < probs[i].k ? probs[i].lanes : probs[i].k;
+    MULTI_CK(cudaMalloc(&p.main, size_t(fdp::main_states(W)) * p.lanes * 4), "multi main state");
+    MULTI_CK(cudaMalloc(&p.blk, size_t(fdp::blocked_states(W)) * p.lanes * 4 + 4), "multi blocked state");
+    MULTI_CK(cudaMalloc(&p.acc, sizeof(unsigned long long) * FDP_MAX_LANES), "multi acc");
+    MULTI_CK(cudaMalloc(&p.res, sizeof(uint32_t) * FDP_MAX_LANES), "multi res");
+    MULTI_CK(cudaStreamCreateWithFlags(&p.s, cudaStreamNonBlocking), "multi stream");
+    MULTI_CK(cudaEventCreateWithFlags(&p.done, cudaEventDisableTiming), "multi event");
+  }
+  auto c0 = std::chrono::steady_clock::now();
+  MULTI_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaEventRecord(fork, c->stream);
+  int off = 0;
+  for (int i = 0; i < count && rs == FDP_OK; ++i) {
+    MultiPart &p = parts[size_t(i)];
+    cudaStreamWaitEvent(p.s, fork, 0);
+    for (int done = 0; done < probs[i].k && rs == FDP_OK; done += p.lanes) {
+      const int L = (probs[i].k - done) < p.lanes ? (probs[i].k - done) : p.lanes;
+      rs = fdp_enqueue_pass(c, *p.t, L, probs[i].moduli + done, p.main, p.blk, p.acc, p.res, pinned + off + done,
+                            p.s, &launches);
+    }
+    cudaEventRecord(p.done, p.s);
+    cudaStreamWaitEvent(c->stream, p.done, 0);
+    off += probs[i].k;
+  }
+  cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+  if (rs != FDP_OK) { cleanup(); return rs; }
+  MULTI_CK(ce, "end capture");
+  MULTI_CK(cudaGraphInstantiate(&ge, g, 0), "graph instantiate");
+  const double cap_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - c0).count();
+  cudaEventRecord(c->ev0, c->stream);
+  MULTI_CK(cudaGraphLaunch(ge, c->stream), "graph launch");
+  cudaEventRecord(c->ev1, c->stream);
+  MULTI_CK(cudaStreamSynchronize(c->stream), "multi pass");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  for (int i = 0; i < total_k; ++i) residues_out[i] = pinned[i];
+  if (st) {
+    fdp_run_stats acc{};
+    acc.device_s = ms * 1e-3;
+    acc.capture_s = cap_s;
+    acc.kernel_launches = launches;
+    for (int i = 0; i < count; ++i) {
+      fdp_plan_out po{};
+      fdp_plan(&probs[i], ~0ull, &po);
+      acc.alg_bytes += po.alg_bytes_per_residue * uint64_t(probs[i].k);
+      acc.transitions += po.transitions_per_residue * uint64_t(probs[i].k);
+    }
+    acc.wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *st = acc;
+  }
+  cleanup();
+  return FDP_OK;
+#undef MULTI_CK
 }

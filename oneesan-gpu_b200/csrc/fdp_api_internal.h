@@ -20,7 +20,9 @@ struct fdp_ctx {
   uint32_t *h_res = nullptr;             // residues, pinned host
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   fdp::LaunchCfg cfg;
-  std::mutex mu;
+  std::mutex mu;         // serialises run_sync / apply_cells / time_cells / tuning
+  std::mutex tables_mu;  // guards `tables` (also used by the serving thread)
+  struct fdp_server *server = nullptr;  // request loop (fdp_server_start)
   ~fdp_ctx();
 };
 
@@ -29,3 +31,5 @@ fdp_status fdp_enqueue_pass(fdp_ctx *c, const fdp::DevTables &t, int L, const ui
                             uint32_t *blk, unsigned long long *acc, uint32_t *d_res, uint32_t *h_res,
                             cudaStream_t s, uint64_t *launches);
 void fdp_set_last_error(const char *msg);
+fdp_status fdp_cuda_status(cudaError_t e, const char *what);
+void fdp_server_shutdown(fdp_ctx *c);

@@ -60,6 +60,24 @@ class RunStats(ctypes.Structure):
                 ("alg_bytes", ctypes.c_uint64), ("transitions", ctypes.c_uint64)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_active", ctypes.c_int),
+                ("max_lanes", ctypes.c_int), ("max_bypass_s", ctypes.c_double)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("queue_s", ctypes.c_double), ("run_s", ctypes.c_double), ("latency_s", ctypes.c_double),
+                ("device_s", ctypes.c_double), ("lanes", ctypes.c_int), ("passes", ctypes.c_int),
+                ("state_bytes", ctypes.c_uint64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("queued", ctypes.c_uint64), ("running", ctypes.c_uint64), ("pool_bytes", ctypes.c_uint64),
+                ("bytes_in_use", ctypes.c_uint64), ("peak_bytes_in_use", ctypes.c_uint64),
+                ("peak_running", ctypes.c_int)]
+
+
 _lib = None
 
 
@@ -84,6 +102,13 @@ def lib() -> ctypes.CDLL:
     L.fdp_time_cells.argtypes = [c_vp, P(Problem), c_int, P(ctypes.c_double)]
     L.fdp_set_tuning.argtypes = [c_vp, P(Tuning)]
     L.fdp_get_tuning.argtypes = [c_vp, P(Tuning)]
+    L.fdp_run_multi_sync.argtypes = [c_vp, P(Problem), c_int, P(c_u32), P(RunStats)]
+    L.fdp_server_start.argtypes = [c_vp, P(ServerConfig)]
+    L.fdp_server_stop.argtypes = [c_vp]
+    L.fdp_submit.argtypes = [c_vp, P(Problem), P(c_u64)]
+    L.fdp_poll.argtypes = [c_vp, c_u64, P(c_u32), P(RequestInfo)]
+    L.fdp_wait.argtypes = [c_vp, c_u64, c_int, P(c_u32), P(RequestInfo)]
+    L.fdp_server_get_stats.argtypes = [c_vp, P(ServerStats)]
     L.fdp_rank_words.argtypes = [c_vp, c_int, c_vp, c_vp, c_u64, c_vp]
     L.fdp_unrank_words.argtypes = [c_vp, c_int, c_vp, c_vp, c_u64, c_vp]
     L.fdp_ternary_index.argtypes = [c_vp, c_vp, c_vp, c_u64, c_vp]
@@ -196,6 +221,22 @@ class Engine:
         _check(lib().fdp_run_sync(self._ctx, ctypes.byref(pr), out, ctypes.byref(st)), "fdp_run_sync")
         return Result([int(x) for x in out], st)
 
+    def residues_multi(self, problems, lanes: int | None = None):
+        """Several (n, moduli) problems in one captured CUDA graph; returns
+        ([residues of each problem], RunStats)."""
+        keep = [_u32_array(m) for _, m in problems]
+        arr = (Problem * len(problems))(*[Problem(n, len(m), keep[i], lanes or min(len(m), MAX_LANES))
+                                          for i, (n, m) in enumerate(problems)])
+        total = sum(len(m) for _, m in problems)
+        out = (ctypes.c_uint32 * total)()
+        st = RunStats()
+        _check(lib().fdp_run_multi_sync(self._ctx, arr, len(problems), out, ctypes.byref(st)), "fdp_run_multi_sync")
+        res, off = [], 0
+        for _, m in problems:
+            res.append([int(x) for x in out[off:off + len(m)]])
+            off += len(m)
+        return res, st
+
     def time_cells(self, n: int, moduli: Sequence[int], lanes: int | None = None, rows: int = 1) -> list:
         """Mean CUDA-event duration (ms) of each cell p = 1..n of a row sweep; index 0 unused."""
         mods = _u32_array(moduli)
@@ -212,6 +253,50 @@ class Engine:
         t = Tuning()
         _check(lib().fdp_get_tuning(self._ctx, ctypes.byref(t)), "fdp_get_tuning")
         return {"block": t.block, "grid": t.grid, "split_panels": bool(t.split_panels)}
+
+    # ---- serving -------------------------------------------------------------
+    def server_start(self, hbm_budget_bytes: int, max_active: int = 8, max_lanes: int = 16,
+                     max_bypass_s: float = 30.0) -> None:
+        cfg = ServerConfig(hbm_budget_bytes, max_active, max_lanes, max_bypass_s)
+        _check(lib().fdp_server_start(self._ctx, ctypes.byref(cfg)), "fdp_server_start")
+
+    def server_stop(self) -> None:
+        _check(lib().fdp_server_stop(self._ctx), "fdp_server_stop")
+
+    def submit(self, n: int, moduli: Sequence[int]) -> int:
+        mods = _u32_array(moduli)
+        pr = Problem(n, len(moduli), mods, 1)
+        rid = ctypes.c_uint64()
+        _check(lib().fdp_submit(self._ctx, ctypes.byref(pr), ctypes.byref(rid)), "fdp_submit")
+        self._pending_k = getattr(self, "_pending_k", {})
+        self._pending_k[rid.value] = len(moduli)
+        return rid.value
+
+    def _result(self, rid: int, status: int, out, info):
+        if status == FDP_PENDING or status == FDP_TIMEOUT:
+            return None
+        self._pending_k.pop(rid, None)
+        _check(status, "request")
+        return {"residues": [int(x) for x in out], "queue_s": info.queue_s, "run_s": info.run_s,
+                "latency_s": info.latency_s, "device_s": info.device_s, "lanes": info.lanes,
+                "passes": info.passes, "state_bytes": info.state_bytes}
+
+    def poll(self, rid: int):
+        """Result dict, or None while the request is queued or running."""
+        out = (ctypes.c_uint32 * self._pending_k[rid])()
+        info = RequestInfo()
+        return self._result(rid, lib().fdp_poll(self._ctx, rid, out, ctypes.byref(info)), out, info)
+
+    def wait(self, rid: int, timeout_ms: int = 600000):
+        """Result dict, or None if the bounded wait ran out."""
+        out = (ctypes.c_uint32 * self._pending_k[rid])()
+        info = RequestInfo()
+        return self._result(rid, lib().fdp_wait(self._ctx, rid, timeout_ms, out, ctypes.byref(info)), out, info)
+
+    def server_stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().fdp_server_get_stats(self._ctx, ctypes.byref(st)), "fdp_server_get_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
 
     def apply_cells(self, width: int, p_hi: int, p_lo: int, moduli: Sequence[int], main_ptr: int,
                     block_ptr: int, stream: int = 0) -> None:

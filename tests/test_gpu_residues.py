@@ -49,3 +49,11 @@ def test_lane_counts_agree(engine):
     for lanes in (2, 5, 7, 16):
         assert engine.residues(n, mods, lanes=lanes).residues == plain
     assert plain[0] == orc.residue(n, mods[0])
+
+
+def test_several_grid_sizes_in_one_graph(engine):
+    problems = [(9, P[:3]), (14, P[3:7]), (12, [2, 3, 5]), (17, P[:14]), (6, [P[0]])]
+    got, st = engine.residues_multi(problems)
+    for (n, mods), res in zip(problems, got):
+        assert res == engine.residues(n, mods, lanes=1).residues
+    assert got[0][:1] == [2674633373] and st.kernel_launches > 0 and st.device_s > 0

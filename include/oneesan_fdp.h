@@ -107,10 +107,12 @@ fdp_status fdp_create(fdp_ctx **out, int device);
 void fdp_destroy(fdp_ctx *ctx);
 
 /*
- * Residues of the path count for every modulus of `problem`, synchronously.
- * lanes = 1 runs one modulus per launch sequence (the reference's residue
- * loop, GB.cu:2211-2258); lanes = k runs all moduli through one captured
- * sweep with `lanes` residues per state.  residues_out has k entries.
+ * Residues of the path count for every modulus of `problem` (k <= 64),
+ * synchronously.  The k moduli run in passes of `lanes` residues per state;
+ * all passes are captured into one CUDA graph and run with one launch.
+ * lanes = 1 is the plain one-modulus-per-launch-sequence form (the
+ * reference's residue loop, GB.cu:2211-2258); lanes = k is one batched pass.
+ * residues_out has k entries.
  */
 fdp_status fdp_run_sync(fdp_ctx *ctx, const fdp_problem *problem, uint32_t *residues_out, fdp_run_stats *stats);
 
@@ -219,6 +221,30 @@ fdp_status fdp_poll(fdp_ctx *ctx, uint64_t request_id, uint32_t *residues_out, f
 fdp_status fdp_wait(fdp_ctx *ctx, uint64_t request_id, int timeout_ms, uint32_t *residues_out,
                     fdp_request_info *info);
 fdp_status fdp_server_get_stats(fdp_ctx *ctx, fdp_server_stats *stats);
+
+/*
+ * Autotuner (the reference's scripts/run/autotune.py:157-300 discipline:
+ * admission from the memory plan, then one warm-up and `repeats` timed samples
+ * per candidate, median, and a known-residue check that aborts on a wrong
+ * answer).  Candidates: residues per pass (how the k moduli of the problem
+ * split into passes; problem->lanes is the largest allowed), one launch vs one
+ * launch per lane panel, and the CTA size.  Each sample is a timed row sweep of
+ * the problem's own n on the context's state buffers; the score is the
+ * estimated device seconds per residue.  The winner is applied to the context
+ * (fdp_set_tuning) and returned; json_out (if not NULL) receives every
+ * candidate record as a JSON document of at most json_cap bytes.
+ */
+typedef struct fdp_autotune_result {
+  int lanes;                /* residues per pass                                  */
+  int passes;               /* passes for the problem's k moduli                  */
+  fdp_tuning tuning;        /* block / grid / split_panels                        */
+  double row_ms;            /* median row-sweep time of the winner                */
+  double s_per_residue;     /* estimated device seconds per residue              */
+  double residues_per_hour; /* 3600 / s_per_residue                               */
+  int candidates, rejected_memory;
+} fdp_autotune_result;
+fdp_status fdp_autotune(fdp_ctx *ctx, const fdp_problem *problem, uint64_t hbm_budget_bytes, int repeats,
+                        fdp_autotune_result *out, char *json_out, size_t json_cap);
 
 /* Canonical rank / unrank of frontier words on the device (GB.cu:1568 rank_full). */
 fdp_status fdp_rank_words(fdp_ctx *ctx, int width, const uint64_t *d_words, uint64_t *d_ranks, uint64_t count,

@@ -14,6 +14,8 @@ using fdp::DevTables;
 
 static thread_local std::string g_last_error;
 
+#define FDP_RUN_MAX_MODULI 64
+
 static fdp_status cuda_status(cudaError_t e, const char *what) {
   if (e == cudaSuccess) return FDP_OK;
   g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
@@ -101,7 +103,7 @@ extern "C" fdp_status fdp_create(fdp_ctx **out, int device) {
   fdp_status s = cuda_status(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
   if (s == FDP_OK) s = cuda_status(cudaMalloc(&c->d_acc, sizeof(unsigned long long) * FDP_MAX_LANES), "acc");
   if (s == FDP_OK) s = cuda_status(cudaMalloc(&c->d_res, sizeof(uint32_t) * FDP_MAX_LANES), "res");
-  if (s == FDP_OK) s = cuda_status(cudaMallocHost(&c->h_res, sizeof(uint32_t) * FDP_MAX_LANES), "pinned res");
+  if (s == FDP_OK) s = cuda_status(cudaMallocHost(&c->h_res, sizeof(uint32_t) * FDP_RUN_MAX_MODULI), "pinned res");
   if (s == FDP_OK) s = cuda_status(cudaEventCreate(&c->ev0), "event");
   if (s == FDP_OK) s = cuda_status(cudaEventCreate(&c->ev1), "event");
   if (s != FDP_OK) {
@@ -177,6 +179,10 @@ extern "C" fdp_status fdp_run_sync(fdp_ctx *c, const fdp_problem *pr, uint32_t *
   if (!c || !residues_out) return FDP_ERR_ARGS;
   fdp_status s = check_problem(pr);
   if (s != FDP_OK) return s;
+  if (pr->k > FDP_RUN_MAX_MODULI) {
+    g_last_error = "run_sync: at most 64 moduli per call";
+    return FDP_ERR_ARGS;
+  }
   std::lock_guard<std::mutex> lk(c->mu);
   auto t0 = std::chrono::steady_clock::now();
   FDP_CK(cudaSetDevice(c->device), "cudaSetDevice");
@@ -187,40 +193,41 @@ extern "C" fdp_status fdp_run_sync(fdp_ctx *c, const fdp_problem *pr, uint32_t *
   const uint64_t M = fdp::main_states(W), D = fdp::blocked_states(W);
   if ((s = ensure_buffer(&c->d_main, &c->cap_main, size_t(M) * lanes * 4, "main state")) != FDP_OK) return s;
   if ((s = ensure_buffer(&c->d_blk, &c->cap_blk, size_t(D) * lanes * 4, "blocked state")) != FDP_OK) return s;
+  // Every pass (lanes residues each) is captured into ONE graph, run with one launch.
   fdp_run_stats acc{};
-  for (int done = 0; done < pr->k; done += lanes) {
+  auto c0 = std::chrono::steady_clock::now();
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  FDP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  uint64_t launches = 0;
+  fdp_status es = FDP_OK;
+  for (int done = 0; done < pr->k && es == FDP_OK; done += lanes) {
     const int L = (pr->k - done) < lanes ? (pr->k - done) : lanes;
-    const uint32_t *mods = pr->moduli + done;
-    auto c0 = std::chrono::steady_clock::now();
-    cudaGraph_t g = nullptr;
-    cudaGraphExec_t ge = nullptr;
-    FDP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-    uint64_t launches = 0;
-    fdp_status es = fdp_enqueue_pass(c, *t, L, mods, c->d_main, c->d_blk, c->d_acc, c->d_res, c->h_res,
-                                     c->stream, &launches);
-    cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
-    if (es != FDP_OK) {
-      if (g) cudaGraphDestroy(g);
-      return es;
-    }
-    FDP_CK(ce, "end capture");
-    ce = cudaGraphInstantiate(&ge, g, 0);
-    cudaGraphDestroy(g);
-    FDP_CK(ce, "graph instantiate");
-    acc.capture_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - c0).count();
-    cudaEventRecord(c->ev0, c->stream);
-    ce = cudaGraphLaunch(ge, c->stream);
-    cudaEventRecord(c->ev1, c->stream);
-    cudaError_t se = cudaStreamSynchronize(c->stream);
-    cudaGraphExecDestroy(ge);
-    FDP_CK(ce, "graph launch");
-    FDP_CK(se, "residue pass");
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    acc.device_s += ms * 1e-3;
-    acc.kernel_launches += launches;
-    for (int i = 0; i < L; ++i) residues_out[done + i] = c->h_res[i];
+    es = fdp_enqueue_pass(c, *t, L, pr->moduli + done, c->d_main, c->d_blk, c->d_acc, c->d_res, c->h_res + done,
+                          c->stream, &launches);
   }
+  cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+  if (es != FDP_OK) {
+    if (g) cudaGraphDestroy(g);
+    return es;
+  }
+  FDP_CK(ce, "end capture");
+  ce = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  FDP_CK(ce, "graph instantiate");
+  acc.capture_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - c0).count();
+  cudaEventRecord(c->ev0, c->stream);
+  ce = cudaGraphLaunch(ge, c->stream);
+  cudaEventRecord(c->ev1, c->stream);
+  cudaError_t se = cudaStreamSynchronize(c->stream);
+  cudaGraphExecDestroy(ge);
+  FDP_CK(ce, "graph launch");
+  FDP_CK(se, "residue pass");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  acc.device_s = ms * 1e-3;
+  acc.kernel_launches = launches;
+  for (int i = 0; i < pr->k; ++i) residues_out[i] = c->h_res[i];
   fdp_plan_out po{};
   fdp_plan(pr, ~0ull, &po);
   acc.alg_bytes = po.alg_bytes_per_residue * uint64_t(pr->k);

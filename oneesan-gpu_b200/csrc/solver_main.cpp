@@ -12,6 +12,8 @@
 //
 // Environment:
 //   FDP_LANES=k         residues per pass (1 = plain, default min(#moduli,16))
+//   FDP_AUTOTUNE=1      pick residues per pass, panel strategy and CTA size with
+//                       fdp_autotune before solving (FDP_LANES caps the lanes)
 //   GRIDFP_PLAN_ONLY=1  print PLAN lines and exit 0 without touching a GPU
 //                       (GB.cu:2117-2168)
 #include <stdio.h>
@@ -95,6 +97,19 @@ int main(int argc, char **argv) {
   if ((s = fdp_create(&ctx, 0)) != FDP_OK) {
     fprintf(stderr, "fdp_create: %s\n", fdp_last_error());
     return exit_code(s);
+  }
+  if (const char *e = getenv("FDP_AUTOTUNE"); e && atoi(e) != 0 && n >= 3) {
+    fdp_problem tp{n, int(mods.size()), mods.data(), lanes};
+    fdp_autotune_result ar{};
+    static char js[1 << 16];
+    s = fdp_autotune(ctx, &tp, ~0ull, 2, &ar, js, sizeof(js));
+    if (s != FDP_OK) {
+      fprintf(stderr, "fdp_autotune: %s\n", fdp_last_error());
+      fdp_destroy(ctx);
+      return exit_code(s);
+    }
+    fprintf(stderr, "autotune %s\n", js);
+    lanes = ar.lanes;
   }
   int rc = 0;
   for (size_t done = 0; done < mods.size(); done += size_t(lanes)) {

@@ -54,6 +54,13 @@ class Tuning(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int), ("grid", ctypes.c_int), ("split_panels", ctypes.c_int)]
 
 
+class AutotuneResult(ctypes.Structure):
+    _fields_ = [("lanes", ctypes.c_int), ("passes", ctypes.c_int), ("tuning", Tuning),
+                ("row_ms", ctypes.c_double), ("s_per_residue", ctypes.c_double),
+                ("residues_per_hour", ctypes.c_double), ("candidates", ctypes.c_int),
+                ("rejected_memory", ctypes.c_int)]
+
+
 class RunStats(ctypes.Structure):
     _fields_ = [("wall_s", ctypes.c_double), ("device_s", ctypes.c_double),
                 ("capture_s", ctypes.c_double), ("kernel_launches", ctypes.c_uint64),
@@ -102,6 +109,8 @@ def lib() -> ctypes.CDLL:
     L.fdp_time_cells.argtypes = [c_vp, P(Problem), c_int, P(ctypes.c_double)]
     L.fdp_set_tuning.argtypes = [c_vp, P(Tuning)]
     L.fdp_get_tuning.argtypes = [c_vp, P(Tuning)]
+    L.fdp_autotune.argtypes = [c_vp, P(Problem), c_u64, c_int, P(AutotuneResult), ctypes.c_char_p,
+                               ctypes.c_size_t]
     L.fdp_run_multi_sync.argtypes = [c_vp, P(Problem), c_int, P(c_u32), P(RunStats)]
     L.fdp_server_start.argtypes = [c_vp, P(ServerConfig)]
     L.fdp_server_stop.argtypes = [c_vp]
@@ -220,6 +229,19 @@ class Engine:
         st = RunStats()
         _check(lib().fdp_run_sync(self._ctx, ctypes.byref(pr), out, ctypes.byref(st)), "fdp_run_sync")
         return Result([int(x) for x in out], st)
+
+    def autotune(self, n: int, moduli: Sequence[int], max_lanes: int = MAX_LANES,
+                 hbm_budget_bytes: int = 170 * 10**9, repeats: int = 2) -> dict:
+        """Pick residues-per-pass, panel strategy and CTA size for (n, moduli);
+        the winner is applied to this engine."""
+        import json as _json
+        mods = _u32_array(moduli)
+        pr = Problem(n, len(moduli), mods, max_lanes)
+        res = AutotuneResult()
+        buf = ctypes.create_string_buffer(1 << 16)
+        _check(lib().fdp_autotune(self._ctx, ctypes.byref(pr), hbm_budget_bytes, repeats, ctypes.byref(res), buf,
+                                  len(buf)), "fdp_autotune")
+        return _json.loads(buf.value.decode())
 
     def residues_multi(self, problems, lanes: int | None = None):
         """Several (n, moduli) problems in one captured CUDA graph; returns

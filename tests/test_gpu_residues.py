@@ -57,3 +57,25 @@ def test_several_grid_sizes_in_one_graph(engine):
     for (n, mods), res in zip(problems, got):
         assert res == engine.residues(n, mods, lanes=1).residues
     assert got[0][:1] == [2674633373] and st.kernel_launches > 0 and st.device_s > 0
+
+
+def test_passes_in_one_graph(engine):
+    mods = P[:20] + [2, 3]
+    got = engine.residues(12, mods, lanes=8)  # 3 passes, one graph launch
+    assert got.residues == engine.residues(12, mods, lanes=1).residues
+    assert got.residues[:2] == [orc.residue(12, mods[0]), orc.residue(12, mods[1])]
+
+
+def test_autotune_picks_a_correct_configuration(engine):
+    mods = P[:6]
+    try:
+        rec = engine.autotune(14, mods, max_lanes=6, repeats=1)
+        best = rec["best"]
+        assert rec["known_residue_check"] == "ok"
+        assert 1 <= best["lanes"] <= 6 and best["s_per_residue"] > 0
+        assert engine.get_tuning()["block"] == best["block"]
+        assert {c["lanes"] for c in rec["candidates"]} >= {1, 2, 4, 6}
+        assert engine.residues(14, mods, lanes=best["lanes"]).residues == [orc.residue(14, m) for m in mods[:1]] + \
+            engine.residues(14, mods[1:], lanes=1).residues
+    finally:
+        engine.set_tuning()

@@ -75,6 +75,7 @@ typedef struct fdp_plan_out {
   uint64_t table_bytes;             /* per-width index tables                     */
   uint64_t total_bytes;
   int rows;                         /* row sweeps per residue                     */
+  int bounded_rows;                 /* of which in height-bounded spaces (prefix) */
   int cells_per_row;                /* W - 1                                      */
   uint64_t alg_bytes_per_residue;   /* sum over cells of fdp_cell_bytes            */
   uint64_t transitions_per_residue; /* sum over cells of (M + D)                  */
@@ -162,12 +163,17 @@ fdp_status fdp_time_cells(fdp_ctx *ctx, const fdp_problem *problem, int rows, do
  * multiple of 32); grid: CTAs per launch (0 = sized from occupancy, a multiple
  * of the SM count); split_panels: for lane counts that need several panels,
  * run one launch per panel instead of one launch that stages closure sources
- * in shared memory.  Results never depend on these settings.
+ * in shared memory; bounded_prefix: run row r in the space of words of height
+ * <= r + 1 while that space is much smaller than the full one (the reference's
+ * bounded-height prefix, GB.cu:1825-1838: row r never reaches a higher height),
+ * growing the state in place between rows.  Results never depend on these
+ * settings.
  */
 typedef struct fdp_tuning {
   int block;
   int grid;
   int split_panels;
+  int bounded_prefix;  /* first rows in height-bounded spaces (default 1)       */
 } fdp_tuning;
 fdp_status fdp_set_tuning(fdp_ctx *ctx, const fdp_tuning *tuning);
 fdp_status fdp_get_tuning(fdp_ctx *ctx, fdp_tuning *tuning);

@@ -77,8 +77,20 @@ extern "C" fdp_status fdp_plan(const fdp_problem *pr, uint64_t budget, fdp_plan_
   o.total_bytes = o.state_bytes + o.table_bytes + (1u << 20);
   o.rows = fdp::sweep_rows(W);
   o.cells_per_row = W - 1;
-  o.alg_bytes_per_residue = uint64_t(o.rows) * (W >= 2 ? fdp::row_bytes(W) : 0);
-  o.transitions_per_residue = uint64_t(o.rows) * uint64_t(o.cells_per_row) * fdp::cell_transitions(W);
+  // Rows run in height-bounded spaces first (fdp_set_tuning bounded_prefix),
+  // then in the full space.
+  std::vector<int> caps;
+  if (W >= 4) caps = fdp::bounded_prefix_caps(W);
+  o.bounded_rows = int(caps.size());
+  o.alg_bytes_per_residue = 0;
+  o.transitions_per_residue = 0;
+  for (int cap : caps) {
+    o.alg_bytes_per_residue += fdp::row_bytes(W, cap);
+    o.transitions_per_residue += uint64_t(o.cells_per_row) * fdp::cell_transitions(W, cap);
+  }
+  const int full_rows = o.rows - o.bounded_rows;
+  o.alg_bytes_per_residue += uint64_t(full_rows) * (W >= 2 ? fdp::row_bytes(W) : 0);
+  o.transitions_per_residue += uint64_t(full_rows) * uint64_t(o.cells_per_row) * fdp::cell_transitions(W);
   o.fits = o.total_bytes <= budget ? 1 : 0;
   *out = o;
   return FDP_OK;
@@ -131,15 +143,35 @@ fdp_ctx::~fdp_ctx() {
 
 extern "C" void fdp_destroy(fdp_ctx *ctx) { delete ctx; }
 
-fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const DevTables **out) {
+fdp_status fdp_ctx_tables_cap(fdp_ctx *c, int W, int cap, const DevTables **out) {
   std::lock_guard<std::mutex> lk(c->tables_mu);
-  auto it = c->tables.find(W);
+  const int key = W * 4096 + (cap >= FDP_FULL_CAP ? 4095 : cap);
+  auto it = c->tables.find(key);
   if (it == c->tables.end()) {
     DevTables t;
-    FDP_CK(fdp::upload_tables(W, &t), "upload tables");
-    it = c->tables.emplace(W, t).first;
+    FDP_CK(fdp::upload_tables(W, cap, &t), "upload tables");
+    it = c->tables.emplace(key, t).first;
   }
   *out = &it->second;
+  return FDP_OK;
+}
+
+fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const DevTables **out) {
+  return fdp_ctx_tables_cap(c, W, FDP_FULL_CAP, out);
+}
+
+// Every device table a residue pass of width W reads, uploaded before any
+// stream capture starts (allocation and blocking copies cannot be captured).
+fdp_status fdp_prepare_pass(fdp_ctx *c, int W, const DevTables **full) {
+  fdp_status s = fdp_ctx_tables(c, W, full);
+  if (s != FDP_OK || !c->cfg.bounded_prefix || W < 4) return s;
+  std::vector<int> caps = fdp::bounded_prefix_caps(W);
+  caps.push_back(1);
+  const DevTables *t = nullptr;
+  for (int cap : caps)
+    if ((s = fdp_ctx_tables_cap(c, W, cap, &t)) != FDP_OK) return s;
+  caps.push_back(FDP_FULL_CAP);
+  FDP_CK(fdp::prepare_expand_tables(caps), "expand tables");
   return FDP_OK;
 }
 
@@ -153,17 +185,45 @@ static fdp_status ensure_buffer(uint32_t **buf, size_t *cap, size_t bytes, const
   return FDP_OK;
 }
 
-// Enqueue one whole residue pass (zero, row-0 init, row sweeps, dot product,
-// residue copy to pinned host memory) on `s`.
+// Enqueue one whole residue pass on `s`: the row-0 state, the row sweeps, the
+// first-row dot product and the residue copy to pinned host memory.  With the
+// bounded prefix (c->cfg.bounded_prefix) row 0 is the height-1 space with every
+// coefficient 1 and row r runs in the space of height cap r + 1 while that
+// space is small; the state grows in place between them (the blocked buffer,
+// dead at row boundaries, stages the move).  `blk` must hold D x L words of
+// the full space.
 fdp_status fdp_enqueue_pass(fdp_ctx *c, const DevTables &t, int L, const uint32_t *mods, uint32_t *main,
                             uint32_t *blk, unsigned long long *acc, uint32_t *d_res, uint32_t *h_res,
                             cudaStream_t s, uint64_t *launches) {
   const int W = t.W;
-  const uint64_t M = fdp::main_states(W);
-  FDP_CK(cudaMemsetAsync(main, 0, size_t(M) * L * 4, s), "zero main");
-  FDP_CK(fdp::launch_first_row_init(t, L, main, s), "row-0 init");
-  uint64_t n = 1;
-  for (int row = 1; row <= fdp::sweep_rows(W); ++row)
+  const uint64_t M = fdp::main_states(W), D = fdp::blocked_states(W);
+  uint64_t n = 0;
+  int first_full_row = 1;
+  if (c->cfg.bounded_prefix && W >= 4) {
+    const std::vector<int> caps = fdp::bounded_prefix_caps(W);
+    const DevTables *prev = nullptr;
+    fdp_status st = fdp_ctx_tables_cap(c, W, 1, &prev);
+    if (st != FDP_OK) return st;
+    FDP_CK(fdp::launch_fill_ones(main, fdp::main_states_capped(W, 1) * uint64_t(L), s), "row-0 fill");
+    ++n;
+    for (size_t r = 0; r < caps.size(); ++r) {
+      const DevTables *cur = nullptr;
+      if ((st = fdp_ctx_tables_cap(c, W, caps[r], &cur)) != FDP_OK) return st;
+      FDP_CK(fdp::enqueue_expand(*prev, *cur, L, main, blk, D * uint64_t(L), s, &n), "grow state");
+      for (int p = W - 1; p >= 1; --p) {
+        FDP_CK(fdp::launch_cell(*cur, L, mods, main, blk, p, p == W - 1, false, c->cfg, s), "bounded cell");
+        ++n;
+      }
+      prev = cur;
+    }
+    FDP_CK(fdp::enqueue_expand(*prev, t, L, main, blk, D * uint64_t(L), s, &n), "grow state");
+    first_full_row = int(caps.size()) + 1;
+  } else {
+    FDP_CK(cudaMemsetAsync(main, 0, size_t(M) * L * 4, s), "zero main");
+    FDP_CK(fdp::launch_first_row_init(t, L, main, s), "row-0 init");
+    ++n;
+  }
+  for (int row = first_full_row; row <= fdp::sweep_rows(W); ++row)
     for (int p = W - 1; p >= 1; --p) {
       FDP_CK(fdp::launch_cell(t, L, mods, main, blk, p, p == W - 1, false, c->cfg, s), "cell");
       ++n;
@@ -188,7 +248,7 @@ extern "C" fdp_status fdp_run_sync(fdp_ctx *c, const fdp_problem *pr, uint32_t *
   FDP_CK(cudaSetDevice(c->device), "cudaSetDevice");
   const int W = pr->n + 1;
   const DevTables *t = nullptr;
-  if ((s = fdp_ctx_tables(c, W, &t)) != FDP_OK) return s;
+  if ((s = fdp_prepare_pass(c, W, &t)) != FDP_OK) return s;
   const int lanes = pr->lanes < pr->k ? pr->lanes : pr->k;
   const uint64_t M = fdp::main_states(W), D = fdp::blocked_states(W);
   if ((s = ensure_buffer(&c->d_main, &c->cap_main, size_t(M) * lanes * 4, "main state")) != FDP_OK) return s;
@@ -338,6 +398,7 @@ extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   c->cfg.block = t->block;
   c->cfg.grid = t->grid;
   c->cfg.split_panels = t->split_panels != 0;
+  c->cfg.bounded_prefix = t->bounded_prefix != 0;
   return FDP_OK;
 }
 
@@ -347,6 +408,7 @@ extern "C" fdp_status fdp_get_tuning(fdp_ctx *c, fdp_tuning *t) {
   t->block = c->cfg.block;
   t->grid = c->cfg.grid;
   t->split_panels = c->cfg.split_panels ? 1 : 0;
+  t->bounded_prefix = c->cfg.bounded_prefix ? 1 : 0;
   return FDP_OK;
 }
 
@@ -404,7 +466,7 @@ extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, i
   for (int i = 0; i < count; ++i) {
     MultiPart &p = parts[size_t(i)];
     const int W = probs[i].n + 1;
-    if ((rs = fdp_ctx_tables(c, W, &p.t)) != FDP_OK) { cleanup(); return rs; }
+    if ((rs = fdp_prepare_pass(c, W, &p.t)) != FDP_OK) { cleanup(); return rs; }
     p.lanes = probs[i].lanes < probs[i].k ? probs[i].lanes : probs[i].k;
     MULTI_CK(cudaMalloc(&p.main, size_t(fdp::main_states(W)) * p.lanes * 4), "multi main state");
     MULTI_CK(cudaMalloc(&p.blk, size_t(fdp::blocked_states(W)) * p.lanes * 4 + 4), "multi blocked state");

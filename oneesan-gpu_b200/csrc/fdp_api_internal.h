@@ -27,6 +27,8 @@ struct fdp_ctx {
 };
 
 fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const fdp::DevTables **out);
+fdp_status fdp_ctx_tables_cap(fdp_ctx *c, int W, int cap, const fdp::DevTables **out);
+fdp_status fdp_prepare_pass(fdp_ctx *c, int W, const fdp::DevTables **full);
 fdp_status fdp_enqueue_pass(fdp_ctx *c, const fdp::DevTables &t, int L, const uint32_t *mods, uint32_t *main,
                             uint32_t *blk, unsigned long long *acc, uint32_t *d_res, uint32_t *h_res,
                             cudaStream_t s, uint64_t *launches);

@@ -3,24 +3,39 @@
 
 #include <string.h>
 
+#include <vector>
+
 namespace fdp {
 
-CountTable::CountTable() {
+CountTable::CountTable(int c) : cap(c) {
   memset(H, 0, sizeof(H));
   H[0][0] = 1;
   for (int w = 1; w <= FDP_MAXW; ++w)
-    for (int h = 0; h < FDP_HT; ++h) {
+    for (int h = 0; h < FDP_HT && h <= cap; ++h) {
       uint64_t x = H[w - 1][h];
       if (h > 0) x += H[w - 1][h - 1];
-      if (h + 1 < FDP_HT) x += H[w - 1][h + 1];
+      if (h + 1 < FDP_HT && h + 1 <= cap) x += H[w - 1][h + 1];
       H[w][h] = x;
     }
 }
 
 const CountTable &counts() {
-  static const CountTable t;
+  static const CountTable t(FDP_FULL_CAP);
   return t;
 }
+
+const CountTable &counts_capped(int cap) {
+  static const std::vector<CountTable> tabs = [] {
+    std::vector<CountTable> v;
+    for (int c = 0; c < FDP_HT; ++c) v.emplace_back(c);
+    return v;
+  }();
+  if (cap < 1 || cap >= FDP_HT - 1) return counts();
+  return tabs[size_t(cap)];
+}
+
+uint64_t main_states_capped(int W, int cap) { return counts_capped(cap).at(W, 1); }
+uint64_t blocked_states_capped(int W, int cap) { return counts_capped(cap).at(W - 1, 1); }
 
 uint64_t main_states(int W) { return counts().at(W, 1); }
 uint64_t blocked_states(int W) { return counts().at(W - 1, 1); }
@@ -31,8 +46,8 @@ bool needs_u64(int W) {
 }
 
 template <typename Idx>
-void build_width_tables(int W, WidthTables<Idx> *t) {
-  const CountTable &c = counts();
+void build_width_tables(int W, WidthTables<Idx> *t, int cap) {
+  const CountTable &c = counts_capped(cap);
   memset(t, 0, sizeof(*t));
   for (int w = 0; w <= FDP_MAXW; ++w)
     for (int h = 0; h < FDP_HT; ++h) t->H[w][h] = Idx(c.H[w][h]);
@@ -53,14 +68,14 @@ void build_width_tables(int W, WidthTables<Idx> *t) {
         t->OFF[p][h][pr] = Idx(off);
         int h1 = h + sym_delta(pair_first(pr));
         int h2 = h1 + sym_delta(pair_second(pr));
-        if (h1 >= 0 && h2 >= 0) off += c.at(p - 1, h2);
+        if (h1 >= 0 && h2 >= 0 && h1 <= c.cap && h2 <= c.cap) off += c.at(p - 1, h2);
       }
     }
   (void)W;
 }
 
-template void build_width_tables<uint32_t>(int, WidthTables<uint32_t> *);
-template void build_width_tables<uint64_t>(int, WidthTables<uint64_t> *);
+template void build_width_tables<uint32_t>(int, WidthTables<uint32_t> *, int);
+template void build_width_tables<uint64_t>(int, WidthTables<uint64_t> *, int);
 
 static inline uint32_t mget(uint64_t m, int k) { return uint32_t(m >> (2 * k)) & 3u; }
 static inline uint64_t msetpair(uint64_t m, int p, uint32_t v) {
@@ -76,8 +91,8 @@ static inline uint64_t mshrink(uint64_t m, int k) {
   return ((m & ~mask) >> 2) | (m & mask);
 }
 
-uint64_t rank_word(uint64_t m, int width) {
-  const CountTable &c = counts();
+uint64_t rank_word(uint64_t m, int width, int cap) {
+  const CountTable &c = counts_capped(cap);
   uint64_t r = 0;
   int h = 1;
   for (int pos = width - 1; pos >= 0; --pos) {
@@ -90,8 +105,8 @@ uint64_t rank_word(uint64_t m, int width) {
   return r;
 }
 
-uint64_t unrank_word(uint64_t rank, int width) {
-  const CountTable &c = counts();
+uint64_t unrank_word(uint64_t rank, int width, int cap) {
+  const CountTable &c = counts_capped(cap);
   uint64_t m = 0;
   int h = 1;
   for (int pos = width - 1; pos >= 0; --pos) {
@@ -179,8 +194,9 @@ uint64_t first_row_state(uint64_t mask, int W) {
   return m;
 }
 
-// Prefix counts: words of `len` symbols from height 1 that end at height h.
-static void prefix_counts(int len, uint64_t *P /* FDP_HT */) {
+// Prefix counts: words of `len` symbols from height 1 that end at height h,
+// heights in [0, cap].
+static void prefix_counts(int len, uint64_t *P /* FDP_HT */, int cap) {
   uint64_t Q[FDP_HT];
   for (int h = 0; h < FDP_HT; ++h) P[h] = 0;
   P[1] = 1;
@@ -190,41 +206,52 @@ static void prefix_counts(int len, uint64_t *P /* FDP_HT */) {
       if (!P[h]) continue;
       Q[h] += P[h];
       if (h > 0) Q[h - 1] += P[h];
-      if (h + 1 < FDP_HT) Q[h + 1] += P[h];
+      if (h + 1 < FDP_HT && h + 1 <= cap) Q[h + 1] += P[h];
     }
     for (int h = 0; h < FDP_HT; ++h) P[h] = Q[h];
   }
 }
 
-uint64_t cell_bytes(int W, int p) {
+uint64_t cell_bytes(int W, int p, int cap) {
   // Minimum traffic of one cell of the in-place sweep, one modulus:
   //   reads : every main word (identity words are closure sources), and the
   //           blocked input except at p = W-1, where it is known to be zero;
   //   writes: main words whose value can change (pair LR/NR/NL or N at p;
   //           at p = 1 the pairs NN, LR, NR, RN) and the blocked output
   //           except at p = 1, which produces none.
-  const CountTable &c = counts();
-  uint64_t M = main_states(W), D = blocked_states(W), wm = 0;
+  const CountTable &c = counts_capped(cap);
+  uint64_t M = main_states_capped(W, cap), D = blocked_states_capped(W, cap), wm = 0;
   uint64_t P[FDP_HT];
-  prefix_counts(W - 1 - p, P);
+  prefix_counts(W - 1 - p, P, c.cap);
   for (int h = 0; h < FDP_HT; ++h) {
     if (!P[h]) continue;
+    const uint64_t lr = h + 1 <= c.cap ? c.at(p - 1, h) : 0;  // the LR sub-block
     if (p == 1)  // NN, LR (h = 0) and NR, RN (h = 1): one word each
-      wm += P[h] * ((h == 0 ? 2 : 0) + (h == 1 ? 2 : 0));
+      wm += P[h] * ((h == 0 ? 1 + lr : 0) + (h == 1 ? 2 : 0));
     else
-      wm += P[h] * (c.at(p, h) + c.at(p - 1, h));
+      wm += P[h] * (c.at(p, h) + lr);
   }
   const uint64_t rd = M + (p < W - 1 ? D : 0);
   const uint64_t wr = wm + (p >= 2 ? D : 0);
   return 4 * (rd + wr);
 }
 
-uint64_t row_bytes(int W) {
+uint64_t row_bytes(int W, int cap) {
   uint64_t b = 0;
-  for (int p = W - 1; p >= 1; --p) b += cell_bytes(W, p);
+  for (int p = W - 1; p >= 1; --p) b += cell_bytes(W, p, cap);
   return b;
 }
 
-uint64_t cell_transitions(int W) { return main_states(W) + blocked_states(W); }
+uint64_t cell_transitions(int W, int cap) { return main_states_capped(W, cap) + blocked_states_capped(W, cap); }
+
+std::vector<int> bounded_prefix_caps(int W) {
+  std::vector<int> caps;
+  const double full = double(main_states(W));
+  for (int cap = 2; cap - 1 <= W - 2 && cap < FDP_HT - 2; ++cap) {
+    if (double(main_states_capped(W, cap)) >= 0.95 * full) break;
+    caps.push_back(cap);
+  }
+  return caps;
+}
 
 }  // namespace fdp

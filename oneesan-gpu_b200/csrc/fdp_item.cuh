@@ -40,6 +40,7 @@ struct CellArgs {
   int W, p;
   int blk_in_zero;     // blocked input known to be zero (first cell of a row sweep)
   int blk_out_p1;      // at p = 1 store the (all-zero) blocked output
+  int cap;             // height cap of the state space (FDP_FULL_CAP: unbounded)
 };
 
 struct FirstRowArgs {
@@ -140,6 +141,7 @@ struct Item {
   Idx iRL;     // RL source (c = N, h > 0)
   int c;       // centre symbol 0=N 1=R 2=L
   int hasRL;
+  int hasLR;   // the LR target exists (always, except at the height cap)
   int nc;      // closure predecessors stored in the candidate slots
 };
 
@@ -179,6 +181,7 @@ FDP_HD Item<Idx> decode_item(const CellArgs &a, const CellSmem<Idx> &sm, const I
   it.iA = bm + off[c == 0 ? PR_NN : (c == 1 ? PR_NR : PR_NL)] + r;
   it.iB = bm + off[c == 0 ? PR_LR : (c == 1 ? PR_RN : PR_LN)] + r;
   it.hasRL = (c == 0 && h > 0 && p >= 2) ? 1 : 0;
+  it.hasLR = (c != 0 || h + 1 <= a.cap) ? 1 : 0;
   it.iRL = bm + off[PR_RL] + r;
   int nc = 0;
   if (c == 0) {
@@ -189,7 +192,7 @@ FDP_HD Item<Idx> decode_item(const CellArgs &a, const CellSmem<Idx> &sm, const I
     if (p >= 3) {
       const Idx baseLL = bm + off[PR_LL];
       Idx rem = r, pre2 = 0;
-      int hb = h, depth = 1;
+      int hb = h, depth = 1, mx = h;  // mx: highest height so far (the predecessor sits 2 higher)
       for (int pos = p - 2; pos >= 0 && depth > 0; --pos) {
         const Idx z0 = sm.H[pos][hb];
         if (rem < z0) continue;  // N: no contribution at either height
@@ -201,9 +204,10 @@ FDP_HD Item<Idx> decode_item(const CellArgs &a, const CellSmem<Idx> &sm, const I
           --depth; --hb;
         } else {         // L
           rem -= z1;
-          if (depth == 1) { on_cand(baseLL + pre2 + up2 + rem); ++nc; }
+          if (depth == 1 && mx + 2 <= a.cap) { on_cand(baseLL + pre2 + up2 + rem); ++nc; }
           pre2 += up2 + sm.H[pos][hb + 1];
           ++depth; ++hb;
+          mx = hb > mx ? hb : mx;
         }
       }
     }
@@ -215,7 +219,7 @@ FDP_HD Item<Idx> decode_item(const CellArgs &a, const CellSmem<Idx> &sm, const I
     const Idx offRR = sm.OFF[h + 2][PR_RR] + r;
     uint64_t nn = (hw | (hw >> 1)) & 0x5555555555555555ull;
     Idx S0 = 0, S2 = 0;
-    int ha = h, depth = 1;
+    int ha = h, depth = 1, mx = h;  // mx: highest height below q (the predecessor sits 2 higher)
     while (nn && depth > 0) {
 #if defined(__CUDA_ARCH__)
       const int b = __ffsll((long long)nn) - 1;
@@ -226,10 +230,11 @@ FDP_HD Item<Idx> decode_item(const CellArgs &a, const CellSmem<Idx> &sm, const I
       const int q = p + 1 + (b >> 1);
       if (((hw >> b) & 3u) == SYM_R) {
         const int hbq = ha + 1;
-        if (depth == 1) { on_cand(bm - S0 + S2 + sm.H[q][h] + offRR); ++nc; }
+        if (depth == 1 && mx + 2 <= a.cap) { on_cand(bm - S0 + S2 + sm.H[q][h] + offRR); ++nc; }
         S0 += sm.H[q][hbq];
         S2 += sm.H[q][hbq + 2];
         ha = hbq; ++depth;
+        mx = hbq > mx ? hbq : mx;
       } else {
         const int hbq = ha - 1;
         S0 += sm.H[q][hbq] + (hbq > 0 ? sm.H[q][hbq - 1] : Idx(0));
@@ -285,7 +290,7 @@ FDP_HD void apply_panels_staged(const CellArgs &a, const Item<Idx> &it, const Id
     } else {
       uint32_t x[PW], acc[PW];
       ld_panel<PW>(pm + size_t(it.iA) * PW, x);
-      {
+      if (it.hasLR) {
         uint32_t y[PW];
         ld_panel<PW>(pm + size_t(it.iB) * PW, y);
 #pragma unroll
@@ -409,7 +414,7 @@ FDP_HD void cell_item_one_panel(const CellArgs &a, const CellSmem<Idx> &sm, cons
   const Idx iLR = bm + off[PR_LR] + r;
   uint32_t x[K], acc[K];
   ld_panel<K>(Mn + size_t(iNN) * K, x);
-  {
+  if (h + 1 <= a.cap) {  // the LR target exists below the height cap
     uint32_t y[K];
     ld_panel<K>(Mn + size_t(iLR) * K, y);
 #pragma unroll
@@ -438,7 +443,7 @@ FDP_HD void cell_item_one_panel(const CellArgs &a, const CellSmem<Idx> &sm, cons
   if (p >= 3) {
     const Idx baseLL = bm + off[PR_LL];
     Idx rem = r, pre2 = 0;
-    int hb = h, depth = 1;
+    int hb = h, depth = 1, mx = h;
     for (int pos = p - 2; pos >= 0 && depth > 0; --pos) {
       const Idx z0 = sm.H[pos][hb];
       if (rem < z0) continue;
@@ -450,16 +455,17 @@ FDP_HD void cell_item_one_panel(const CellArgs &a, const CellSmem<Idx> &sm, cons
         --depth; --hb;
       } else {
         rem -= z1;
-        if (depth == 1) add_source(baseLL + pre2 + up2 + rem);
+        if (depth == 1 && mx + 2 <= a.cap) add_source(baseLL + pre2 + up2 + rem);
         pre2 += up2 + sm.H[pos][hb + 1];
         ++depth; ++hb;
+        mx = hb > mx ? hb : mx;
       }
     }
   }
   // RR closures: every R at depth 1 of the high part, flipped to L.
   {
     Idx S0 = 0, S2 = 0;
-    int ha = h, depth = 1;
+    int ha = h, depth = 1, mx = h;
     const Idx offRR = sm.OFF[h + 2][PR_RR] + r;
     uint64_t w = hw;
     for (int q = p + 1; q <= W - 1 && depth > 0; ++q, w >>= 2) {
@@ -467,10 +473,11 @@ FDP_HD void cell_item_one_panel(const CellArgs &a, const CellSmem<Idx> &sm, cons
       if (sy == SYM_N) continue;
       if (sy == SYM_R) {
         const int hbq = ha + 1;
-        if (depth == 1) add_source(bm - S0 + S2 + sm.H[q][h] + offRR);
+        if (depth == 1 && mx + 2 <= a.cap) add_source(bm - S0 + S2 + sm.H[q][h] + offRR);
         S0 += sm.H[q][hbq];
         S2 += sm.H[q][hbq + 2];
         ha = hbq; ++depth;
+        mx = hbq > mx ? hbq : mx;
       } else {
         const int hbq = ha - 1;
         S0 += sm.H[q][hbq] + (hbq > 0 ? sm.H[q][hbq - 1] : Idx(0));

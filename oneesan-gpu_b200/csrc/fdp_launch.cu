@@ -1,6 +1,9 @@
 // Dispatch of the templated kernels, per-width table upload, and the small
 // operator-surface kernels (rank / unrank / ternary index).
+#include <map>
 #include <memory>
+#include <mutex>
+#include <vector>
 
 #include "fdp_host.h"
 #include "fdp_launch.h"
@@ -14,18 +17,19 @@ int device_sm_count() {
   return n;
 }
 
-cudaError_t upload_tables(int W, DevTables *out) {
+cudaError_t upload_tables(int W, int cap, DevTables *out) {
   out->W = W;
+  out->cap = cap;
   out->u64 = needs_u64(W);
   cudaError_t e;
   if (out->u64) {
     auto t = std::make_unique<WidthTables<uint64_t>>();
-    build_width_tables<uint64_t>(W, t.get());
+    build_width_tables<uint64_t>(W, t.get(), cap);
     if ((e = cudaMalloc(&out->ptr, sizeof(*t))) != cudaSuccess) return e;
     return cudaMemcpy(out->ptr, t.get(), sizeof(*t), cudaMemcpyHostToDevice);
   }
   auto t = std::make_unique<WidthTables<uint32_t>>();
-  build_width_tables<uint32_t>(W, t.get());
+  build_width_tables<uint32_t>(W, t.get(), cap);
   if ((e = cudaMalloc(&out->ptr, sizeof(*t))) != cudaSuccess) return e;
   return cudaMemcpy(out->ptr, t.get(), sizeof(*t), cudaMemcpyHostToDevice);
 }
@@ -74,11 +78,12 @@ cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_
   a.tables = t.ptr;
   a.main = main;
   a.blk = blk;
-  a.items = blocked_states(t.W);
-  a.mstates = main_states(t.W);
+  a.items = blocked_states_capped(t.W, t.cap);
+  a.mstates = main_states_capped(t.W, t.cap);
   for (int i = 0; i < K; ++i) a.mod[i] = mods[i];
   a.W = t.W;
   a.p = p;
+  a.cap = t.cap;
   a.blk_in_zero = blk_in_zero ? 1 : 0;
   a.blk_out_p1 = blk_out_p1 ? 1 : 0;
   const bool one_panel = (K == 1 || K == 2 || K == 4 || K == 8);
@@ -135,6 +140,115 @@ cudaError_t launch_first_row_dot(const DevTables &t, int K, const uint32_t *mods
   for (int i = 0; i < K; ++i) a.mod[i] = mods[i];
   finalize_residues_kernel<<<1, 32, 0, s>>>(acc, residues, a, K);
   return cudaGetLastError();
+}
+
+// ---- height-bounded prefix: row-0 fill and in-place expansion ------------------
+__global__ void fill_ones_kernel(uint32_t *a, uint64_t words) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < words; i += uint64_t(gridDim.x) * blockDim.x)
+    a[i] = 1u;
+}
+
+cudaError_t launch_fill_ones(uint32_t *a, uint64_t words, cudaStream_t s) {
+  if (!words) return cudaSuccess;
+  uint64_t g = (words + 255) / 256, cap = uint64_t(device_sm_count()) * 8;
+  fill_ones_kernel<<<unsigned(g < cap ? g : cap), 256, 0, s>>>(a, words);
+  return cudaGetLastError();
+}
+
+struct CapTable {
+  unsigned long long H[FDP_MAXW + 1][FDP_HT];
+};
+
+// dst[rank_to(w_i) * pw + l] = tmp[(i - lo) * pw + l] for the words w_i of the
+// `from` space with index i in [lo, hi).
+__global__ void expand_scatter_kernel(const CapTable *from, const CapTable *to, int W, uint64_t lo, uint64_t hi,
+                                      int pw, const uint32_t *tmp, uint32_t *dst) {
+  __shared__ unsigned long long sf[FDP_MAXW + 1][FDP_HT], st[FDP_MAXW + 1][FDP_HT];
+  for (int i = threadIdx.x; i < (FDP_MAXW + 1) * FDP_HT; i += blockDim.x) {
+    (&sf[0][0])[i] = (&from->H[0][0])[i];
+    (&st[0][0])[i] = (&to->H[0][0])[i];
+  }
+  __syncthreads();
+  for (uint64_t i = lo + uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < hi; i += uint64_t(gridDim.x) * blockDim.x) {
+    unsigned long long r = i;
+    uint64_t m = 0;
+    int h = 1;
+    for (int pos = W - 1; pos >= 0; --pos) {  // unrank in the `from` space
+      unsigned long long z = sf[pos][h];
+      if (r < z) continue;
+      r -= z;
+      z = h > 0 ? sf[pos][h - 1] : 0ull;
+      if (r < z) { m |= uint64_t(SYM_R) << (2 * pos); --h; continue; }
+      r -= z;
+      m |= uint64_t(SYM_L) << (2 * pos);
+      ++h;
+    }
+    const unsigned long long j = rank_dev<unsigned long long>(m, W, st);
+    for (int l = 0; l < pw; ++l) dst[size_t(j) * pw + l] = tmp[size_t(i - lo) * pw + l];
+  }
+}
+
+static const CapTable *cap_table(int cap) {
+  static std::map<std::pair<int, int>, CapTable *> tabs;  // (device, cap) -> table
+  static std::mutex mu;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_pair(dev, cap);
+  auto it = tabs.find(key);
+  if (it != tabs.end()) return it->second;
+  CapTable h;
+  const CountTable &c = counts_capped(cap);
+  for (int w = 0; w <= FDP_MAXW; ++w)
+    for (int k = 0; k < FDP_HT; ++k) h.H[w][k] = c.H[w][k];
+  CapTable *p = nullptr;
+  if (cudaMalloc(&p, sizeof(h)) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(p, &h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+  tabs[key] = p;
+  return p;
+}
+
+cudaError_t prepare_expand_tables(const std::vector<int> &caps) {
+  for (int cap : caps)
+    if (!cap_table(cap)) return cudaErrorMemoryAllocation;
+  return cudaSuccess;
+}
+
+cudaError_t enqueue_expand(const DevTables &from, const DevTables &to, int K, uint32_t *a, uint32_t *tmp,
+                           uint64_t tmp_words, cudaStream_t s, uint64_t *launches) {
+  const int W = from.W;
+  const uint64_t Nf = main_states_capped(W, from.cap), Nt = main_states_capped(W, to.cap);
+  const CapTable *tf = cap_table(from.cap), *tt = cap_table(to.cap);
+  if (!tf || !tt) return cudaErrorMemoryAllocation;
+  // Panels (first lane, width) of the K-lane layout, last panel first.
+  std::vector<std::pair<int, int>> panels;
+  for (int l0 = 0; l0 < K;) {
+    const int pw = (K - l0 >= 8) ? 8 : (K - l0 >= 4) ? 4 : (K - l0 >= 2) ? 2 : 1;
+    panels.push_back({l0, pw});
+    l0 += pw;
+  }
+  for (size_t pi = panels.size(); pi-- > 0;) {
+    const int l0 = panels[pi].first, pw = panels[pi].second;
+    uint32_t *src = a + size_t(l0) * Nf, *dst = a + size_t(l0) * Nt;
+    const uint64_t chunk = tmp_words / uint64_t(pw);
+    if (!chunk) return cudaErrorInvalidValue;
+    uint64_t hi = Nf, top = Nt;  // `top`: new index of the chunk above (already placed)
+    while (hi > 0) {
+      const uint64_t lo = hi > chunk ? hi - chunk : 0;
+      const uint64_t nlo = rank_word(unrank_word(lo, W, from.cap), W, to.cap);
+      cudaError_t e = cudaMemcpyAsync(tmp, src + size_t(lo) * pw, size_t(hi - lo) * pw * 4, cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(dst + size_t(nlo) * pw, 0, size_t(top - nlo) * pw * 4, s)) != cudaSuccess) return e;
+      const uint64_t n = hi - lo;
+      uint64_t g = (n + 255) / 256, gc = uint64_t(device_sm_count()) * 8;
+      expand_scatter_kernel<<<unsigned(g < gc ? g : gc), 256, 0, s>>>(tf, tt, W, lo, hi, pw, tmp, dst);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      if (launches) ++*launches;
+      top = nlo;
+      hi = lo;
+    }
+  }
+  return cudaSuccess;
 }
 
 // ---- operator surface: canonical rank / unrank / ternary index ---------------

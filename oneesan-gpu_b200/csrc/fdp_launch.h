@@ -4,25 +4,29 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "fdp_item.cuh"
 
 namespace fdp {
 
 constexpr int kMaxLanes = 16;  // K = 1..16 residues interleaved per state
 
-// Per-width device table blob.
+// Per-(width, height cap) device table blob.
 struct DevTables {
   void *ptr = nullptr;
   bool u64 = false;
   int W = 0;
+  int cap = 1000;  // FDP_FULL_CAP: the full space
 };
-cudaError_t upload_tables(int W, DevTables *out);
+cudaError_t upload_tables(int W, int cap, DevTables *out);
 void free_tables(DevTables *t);
 
 struct LaunchCfg {
   int block = 256;
   int grid = 0;              // 0: sized from occupancy (a multiple of the SM count)
   bool split_panels = false; // several panels: one single-panel launch per panel
+  bool bounded_prefix = true;  // first rows in height-bounded spaces
 };
 
 template <typename Idx, int K>
@@ -38,6 +42,20 @@ cudaError_t launch_first_row_init(const DevTables &t, int K, uint32_t *main, cud
 // acc[k] += sum over first-row states of main[.][k]; then residues[k] = acc[k] mod p_k.
 cudaError_t launch_first_row_dot(const DevTables &t, int K, const uint32_t *mods, const uint32_t *main,
                                  unsigned long long *acc, uint32_t *residues, cudaStream_t s);
+
+// Every word of the K lanes of the first N states set to 1 (row 0 in the
+// height-1 space: every such word is a first-row state with coefficient 1).
+cudaError_t launch_fill_ones(uint32_t *a, uint64_t words, cudaStream_t s);
+// Move a K-lane state vector, in place, from the space `from` to the larger
+// space `to` of the same width (ranks only grow), staging through `tmp`
+// (tmp_words words, not overlapping `a`); words of `to` outside the image are
+// zeroed.
+cudaError_t enqueue_expand(const DevTables &from, const DevTables &to, int K, uint32_t *a, uint32_t *tmp,
+                           uint64_t tmp_words, cudaStream_t s, uint64_t *launches = nullptr);
+
+// Upload (once per device) the count tables enqueue_expand uses for these caps;
+// must run outside stream capture.
+cudaError_t prepare_expand_tables(const std::vector<int> &caps);
 
 // Operator-surface helpers.
 cudaError_t launch_rank_words(int width, const uint64_t *words, uint64_t *ranks, uint64_t count, cudaStream_t s);

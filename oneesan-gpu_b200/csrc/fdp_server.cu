@@ -134,7 +134,7 @@ struct fdp_server {
     const int slot = j->slot;
     cudaStream_t s = streams[size_t(slot)];
     const fdp::DevTables *t = nullptr;
-    fdp_status st = fdp_ctx_tables(ctx, j->n + 1, &t);
+    fdp_status st = fdp_prepare_pass(ctx, j->n + 1, &t);
     if (st != FDP_OK) return st;
     const int W = j->n + 1;
     const uint64_t M = fdp::main_states(W);

@@ -45,13 +45,14 @@ class PlanOut(ctypes.Structure):
                 ("main_states", ctypes.c_uint64), ("blocked_states", ctypes.c_uint64),
                 ("state_bytes", ctypes.c_uint64), ("scratch_bytes", ctypes.c_uint64),
                 ("table_bytes", ctypes.c_uint64), ("total_bytes", ctypes.c_uint64),
-                ("rows", ctypes.c_int), ("cells_per_row", ctypes.c_int),
+                ("rows", ctypes.c_int), ("bounded_rows", ctypes.c_int), ("cells_per_row", ctypes.c_int),
                 ("alg_bytes_per_residue", ctypes.c_uint64),
                 ("transitions_per_residue", ctypes.c_uint64), ("fits", ctypes.c_int)]
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("block", ctypes.c_int), ("grid", ctypes.c_int), ("split_panels", ctypes.c_int)]
+    _fields_ = [("block", ctypes.c_int), ("grid", ctypes.c_int), ("split_panels", ctypes.c_int),
+                ("bounded_prefix", ctypes.c_int)]
 
 
 class AutotuneResult(ctypes.Structure):
@@ -267,14 +268,16 @@ class Engine:
         _check(lib().fdp_time_cells(self._ctx, ctypes.byref(pr), rows, out), "fdp_time_cells")
         return [float(x) for x in out]
 
-    def set_tuning(self, block: int = 256, grid: int = 0, split_panels: bool = False) -> None:
-        t = Tuning(block, grid, 1 if split_panels else 0)
+    def set_tuning(self, block: int = 256, grid: int = 0, split_panels: bool = False,
+                   bounded_prefix: bool = True) -> None:
+        t = Tuning(block, grid, 1 if split_panels else 0, 1 if bounded_prefix else 0)
         _check(lib().fdp_set_tuning(self._ctx, ctypes.byref(t)), "fdp_set_tuning")
 
     def get_tuning(self) -> dict:
         t = Tuning()
         _check(lib().fdp_get_tuning(self._ctx, ctypes.byref(t)), "fdp_get_tuning")
-        return {"block": t.block, "grid": t.grid, "split_panels": bool(t.split_panels)}
+        return {"block": t.block, "grid": t.grid, "split_panels": bool(t.split_panels),
+                "bounded_prefix": bool(t.bounded_prefix)}
 
     # ---- serving -------------------------------------------------------------
     def server_start(self, hbm_budget_bytes: int, max_active: int = 8, max_lanes: int = 16,

@@ -99,7 +99,8 @@ def test_tuning_never_changes_results(engine):
     try:
         for block, grid, split in ((128, 0, True), (64, 37, False), (256, 1, True), (96, 0, False)):
             engine.set_tuning(block=block, grid=grid, split_panels=split)
-            assert engine.get_tuning() == {"block": block, "grid": grid, "split_panels": split}
+            assert engine.get_tuning() == {"block": block, "grid": grid, "split_panels": split,
+                                           "bounded_prefix": True}
             _run(engine, 12, 11, 1, [MODS[i % 3] for i in range(14)], seed=block + grid)
     finally:
         engine.set_tuning()

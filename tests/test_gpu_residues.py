@@ -79,3 +79,15 @@ def test_autotune_picks_a_correct_configuration(engine):
             engine.residues(14, mods[1:], lanes=1).residues
     finally:
         engine.set_tuning()
+
+
+def test_bounded_prefix_equals_full_rows(engine):
+    try:
+        for n, mods in ((4, P[:1]), (9, P[:2]), (15, P[:5]), (16, P[:14])):
+            engine.set_tuning(bounded_prefix=False)
+            full = engine.residues(n, mods, lanes=len(mods)).residues
+            engine.set_tuning(bounded_prefix=True)
+            assert engine.residues(n, mods, lanes=len(mods)).residues == full, n
+            assert engine.residues(n, mods, lanes=1).residues == full, n
+    finally:
+        engine.set_tuning()

@@ -252,6 +252,35 @@ typedef struct fdp_autotune_result {
 fdp_status fdp_autotune(fdp_ctx *ctx, const fdp_problem *problem, uint64_t hbm_budget_bytes, int repeats,
                         fdp_autotune_result *out, char *json_out, size_t json_cap);
 
+/*
+ * Factorized transfer map: the cell operator (or two consecutive cells when
+ * `paired`) as a CSR matrix of predecessor indices over the index space
+ * [0, M) main + [M, M+D) blocked of one width, built on the device (count,
+ * scan, fill, and a check that the fill pass agrees with the count pass) and
+ * applied out of place: out_main = in_main + T x, out_block = T x.  Replaces
+ * factor_transfer::{counts,fill,verify,apply}_kernel
+ * (src/cuda/b300/factor_transfer_map.cuh:40-68) and its batched apply
+ * (factor_transfer_batch.cuh:13-47); lanes follow the panel layout.
+ * Widths whose M + D exceeds 2^32 are rejected (32-bit columns).
+ */
+typedef struct fdp_transfer_map fdp_transfer_map;
+fdp_status fdp_transfer_map_build(fdp_ctx *ctx, int width, int p, int paired, fdp_transfer_map **out);
+fdp_status fdp_transfer_map_info(const fdp_transfer_map *map, uint64_t *rows, uint64_t *edges,
+                                 uint64_t *device_bytes);
+fdp_status fdp_transfer_map_apply(fdp_ctx *ctx, const fdp_transfer_map *map, int lanes, const uint32_t *moduli,
+                                  const uint32_t *d_in_main, const uint32_t *d_in_block, uint32_t *d_out_main,
+                                  uint32_t *d_out_block, void *stream);
+void fdp_transfer_map_destroy(fdp_transfer_map *map);
+
+/*
+ * Two consecutive cells p, p-1 fused by recursive pull, out of place, without
+ * storing the intermediate vector or a matrix (the reverse2 kernels,
+ * R2.cu:1116-1155).  Same result as fdp_apply_cells(p, p-1).
+ */
+fdp_status fdp_reverse2_apply(fdp_ctx *ctx, int width, int p, int lanes, const uint32_t *moduli,
+                              const uint32_t *d_in_main, const uint32_t *d_in_block, uint32_t *d_out_main,
+                              uint32_t *d_out_block, void *stream);
+
 /* Canonical rank / unrank of frontier words on the device (GB.cu:1568 rank_full). */
 fdp_status fdp_rank_words(fdp_ctx *ctx, int width, const uint64_t *d_words, uint64_t *d_ranks, uint64_t count,
                           void *stream);

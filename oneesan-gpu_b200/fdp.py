@@ -112,6 +112,12 @@ def lib() -> ctypes.CDLL:
     L.fdp_get_tuning.argtypes = [c_vp, P(Tuning)]
     L.fdp_autotune.argtypes = [c_vp, P(Problem), c_u64, c_int, P(AutotuneResult), ctypes.c_char_p,
                                ctypes.c_size_t]
+    L.fdp_transfer_map_build.argtypes = [c_vp, c_int, c_int, c_int, P(c_vp)]
+    L.fdp_transfer_map_info.argtypes = [c_vp, P(c_u64), P(c_u64), P(c_u64)]
+    L.fdp_transfer_map_apply.argtypes = [c_vp, c_vp, c_int, P(c_u32), c_vp, c_vp, c_vp, c_vp, c_vp]
+    L.fdp_transfer_map_destroy.argtypes = [c_vp]
+    L.fdp_transfer_map_destroy.restype = None
+    L.fdp_reverse2_apply.argtypes = [c_vp, c_int, c_int, c_int, P(c_u32), c_vp, c_vp, c_vp, c_vp, c_vp]
     L.fdp_run_multi_sync.argtypes = [c_vp, P(Problem), c_int, P(c_u32), P(RunStats)]
     L.fdp_server_start.argtypes = [c_vp, P(ServerConfig)]
     L.fdp_server_stop.argtypes = [c_vp]
@@ -323,6 +329,19 @@ class Engine:
         _check(lib().fdp_server_get_stats(self._ctx, ctypes.byref(st)), "fdp_server_get_stats")
         return {f: getattr(st, f) for f, _ in ServerStats._fields_}
 
+    # ---- operator variants ---------------------------------------------------
+    def transfer_map(self, width: int, p: int, paired: bool = False) -> "TransferMap":
+        h = ctypes.c_void_p()
+        _check(lib().fdp_transfer_map_build(self._ctx, width, p, 1 if paired else 0, ctypes.byref(h)),
+               "fdp_transfer_map_build")
+        return TransferMap(self, h)
+
+    def reverse2_apply(self, width: int, p: int, moduli: Sequence[int], in_main: int, in_block: int,
+                       out_main: int, out_block: int, stream: int = 0) -> None:
+        mods = _u32_array(moduli)
+        _check(lib().fdp_reverse2_apply(self._ctx, width, p, len(moduli), mods, in_main, in_block, out_main,
+                                        out_block, stream), "fdp_reverse2_apply")
+
     def apply_cells(self, width: int, p_hi: int, p_lo: int, moduli: Sequence[int], main_ptr: int,
                     block_ptr: int, stream: int = 0) -> None:
         mods = _u32_array(moduli)
@@ -337,3 +356,33 @@ class Engine:
 
     def ternary_index(self, codes_ptr: int, index_ptr: int, count: int, stream: int = 0) -> None:
         _check(lib().fdp_ternary_index(self._ctx, codes_ptr, index_ptr, count, stream), "fdp_ternary_index")
+
+
+class TransferMap:
+    """A CSR transfer map on the device (fdp_transfer_map_*)."""
+
+    def __init__(self, engine: Engine, handle):
+        self._eng, self._h = engine, handle
+
+    def info(self) -> dict:
+        r, e, b = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().fdp_transfer_map_info(self._h, ctypes.byref(r), ctypes.byref(e), ctypes.byref(b)),
+               "fdp_transfer_map_info")
+        return {"rows": r.value, "edges": e.value, "device_bytes": b.value}
+
+    def apply(self, moduli: Sequence[int], in_main: int, in_block: int, out_main: int, out_block: int,
+              stream: int = 0) -> None:
+        mods = _u32_array(moduli)
+        _check(lib().fdp_transfer_map_apply(self._eng._ctx, self._h, len(moduli), mods, in_main, in_block,
+                                            out_main, out_block, stream), "fdp_transfer_map_apply")
+
+    def close(self) -> None:
+        if self._h:
+            lib().fdp_transfer_map_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -123,7 +123,7 @@ fdp_status fdp_run_sync(fdp_ctx *ctx, const fdp_problem *problem, uint32_t *resi
  * end, and the graph runs with a single launch, so the problems overlap on the
  * GPU.  residues_out receives the residues of problem 0, then problem 1, ...
  * (sum of k entries).  stats covers the whole graph.  No counterpart in the
- * reference, which runs one n per binary (SURVEY north star "batched" form).
+ * reference, which runs one n per binary (the batched form of this engine).
  */
 fdp_status fdp_run_multi_sync(fdp_ctx *ctx, const fdp_problem *problems, int count, uint32_t *residues_out,
                               fdp_run_stats *stats);
@@ -166,21 +166,27 @@ fdp_status fdp_time_cells(fdp_ctx *ctx, const fdp_problem *problem, int rows, do
  * in shared memory; bounded_prefix: run row r in the space of words of height
  * <= r + 1 while that space is much smaller than the full one (the reference's
  * bounded-height prefix, GB.cu:1825-1838: row r never reaches a higher height),
- * growing the state in place between rows.  Results never depend on these
- * settings.
+ * growing the state in place between rows.  lane_items: each warp of the cell
+ * kernel takes chunks of 32 * lane_items consecutive blocked states (0 = the
+ * default, 8); share_min: when a cell's high prefix is at least this many
+ * symbols long, the symbols a whole chunk shares are decoded once per chunk
+ * (0 = the default, 4; a value above the width never shares).  Results never
+ * depend on these settings.
  */
 typedef struct fdp_tuning {
   int block;
   int grid;
   int split_panels;
   int bounded_prefix;  /* first rows in height-bounded spaces (default 1)       */
+  int lane_items;      /* states per lane of a warp chunk, 0..64 (0: default)   */
+  int share_min;       /* shortest prefix decoded once per chunk (0: default)   */
 } fdp_tuning;
 fdp_status fdp_set_tuning(fdp_ctx *ctx, const fdp_tuning *tuning);
 fdp_status fdp_get_tuning(fdp_ctx *ctx, fdp_tuning *tuning);
 
 /*
  * Serving: a request loop with continuous batching.  No counterpart in the
- * reference, which runs one process per job (SURVEY north star "served" form).
+ * reference, which runs one process per job (the served form of this engine).
  *
  * fdp_server_start reserves hbm_budget_bytes of device memory once and starts
  * a scheduler thread.  Requests (n, moduli) queue in arrival order; a request

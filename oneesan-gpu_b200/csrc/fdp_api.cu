@@ -359,7 +359,10 @@ extern "C" fdp_status fdp_time_cells(fdp_ctx *c, const fdp_problem *pr, int rows
   if ((s = ensure_buffer(&c->d_blk, &c->cap_blk, size_t(D) * L * 4, "blocked state")) != FDP_OK) return s;
   std::vector<cudaEvent_t> ev(size_t(rows) * W * 2);
   for (auto &e : ev) FDP_CK(cudaEventCreate(&e), "event");
-  fdp_status rs = FDP_OK;
+  // One untimed launch first: the first launch of a kernel variant also loads
+  // its module and sets its shared-memory limit.
+  fdp_status rs = cuda_status(
+      fdp::launch_cell(*t, L, pr->moduli, c->d_main, c->d_blk, W - 1, true, false, c->cfg, c->stream), "cell");
   for (int r = 0; r < rows && rs == FDP_OK; ++r)
     for (int p = W - 1; p >= 1 && rs == FDP_OK; --p) {
       cudaEventRecord(ev[(size_t(r) * W + p) * 2], c->stream);
@@ -390,8 +393,9 @@ void fdp_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 
 extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   if (!c || !t) return FDP_ERR_ARGS;
-  if (t->block < 64 || t->block > 256 || t->block % 32 || t->grid < 0) {
-    g_last_error = "tuning: block must be a multiple of 32 in 64..256 and grid >= 0";
+  if (t->block < 64 || t->block > 256 || t->block % 32 || t->grid < 0 || t->lane_items < 0 || t->lane_items > 64 ||
+      t->share_min < 0) {
+    g_last_error = "tuning: block must be a multiple of 32 in 64..256, grid >= 0, lane_items 0..64, share_min >= 0";
     return FDP_ERR_ARGS;
   }
   std::lock_guard<std::mutex> lk(c->mu);
@@ -399,6 +403,8 @@ extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   c->cfg.grid = t->grid;
   c->cfg.split_panels = t->split_panels != 0;
   c->cfg.bounded_prefix = t->bounded_prefix != 0;
+  c->cfg.lane_items = t->lane_items > 0 ? t->lane_items : fdp::LaunchCfg{}.lane_items;
+  c->cfg.share_min = t->share_min > 0 ? t->share_min : fdp::LaunchCfg{}.share_min;
   return FDP_OK;
 }
 
@@ -409,6 +415,8 @@ extern "C" fdp_status fdp_get_tuning(fdp_ctx *c, fdp_tuning *t) {
   t->grid = c->cfg.grid;
   t->split_panels = c->cfg.split_panels ? 1 : 0;
   t->bounded_prefix = c->cfg.bounded_prefix ? 1 : 0;
+  t->lane_items = c->cfg.lane_items;
+  t->share_min = c->cfg.share_min;
   return FDP_OK;
 }
 

@@ -28,7 +28,8 @@ cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t 
     configured_block = cfg.block;
   }
   int grid = cfg.grid > 0 ? cfg.grid : device_sm_count() * per_sm;
-  const uint64_t need = (a.items + cfg.block - 1) / cfg.block;
+  const uint64_t per_block = uint64_t(cfg.block) * uint64_t(a.lane_items < 1 ? 1 : a.lane_items);
+  const uint64_t need = (a.items + per_block - 1) / per_block;
   if (uint64_t(grid) > need) grid = int(need ? need : 1);
   cell_kernel<Idx, K><<<grid, cfg.block, smem, s>>>(a);
   return cudaGetLastError();

@@ -41,6 +41,8 @@ struct CellArgs {
   int blk_in_zero;     // blocked input known to be zero (first cell of a row sweep)
   int blk_out_p1;      // at p = 1 store the (all-zero) blocked output
   int cap;             // height cap of the state space (FDP_FULL_CAP: unbounded)
+  int lane_items;      // items per lane of one warp chunk (the chunk is 32 * lane_items indices)
+  int share_prefix;    // decode the prefix a warp chunk shares once per chunk
 };
 
 struct FirstRowArgs {
@@ -58,16 +60,6 @@ template <int K, int L0>
 struct PanelW {
   static constexpr int value = (K - L0 >= 8) ? 8 : (K - L0 >= 4) ? 4 : ((K - L0 >= 2) ? 2 : 1);
 };
-
-template <int K>
-constexpr int panel_count() {
-  int n = 0;
-  for (int l = 0; l < K;) {
-    l += (K - l >= 8) ? 8 : (K - l >= 4) ? 4 : (K - l >= 2) ? 2 : 1;
-    ++n;
-  }
-  return n;
-}
 
 template <int PW>
 FDP_HD void ld_panel(const uint32_t *p, uint32_t *x) {
@@ -122,6 +114,48 @@ FDP_HD void st_lanes(uint32_t *base, size_t N, size_t s, const uint32_t *x) {
   }
 }
 
+// Spans: runs of consecutive panels holding at most 8 lanes together (K = 14:
+// {0-7}, {8-13}).  The cell kernel reads and writes a state one span at a
+// time and issues all loads of a span before it uses any of them, so a lane
+// count of several small panels costs no more dependent load phases than one
+// of 8-wide panels.
+FDP_HD constexpr int span_end_of(int K, int L0) {
+  int l = L0, w = 0;
+  while (l < K) {
+    const int pw = (K - l >= 8) ? 8 : (K - l >= 4) ? 4 : ((K - l >= 2) ? 2 : 1);
+    if (w + pw > 8) break;
+    w += pw;
+    l += pw;
+  }
+  return l;
+}
+
+template <int K>
+constexpr int span_count() {
+  int n = 0;
+  for (int l = 0; l < K; l = span_end_of(K, l)) ++n;
+  return n;
+}
+
+// Lanes [L0, LE) of state s (LE a span end) into x[0 .. LE-L0).
+template <int K, int L0, int LE, int X0 = L0>
+FDP_HD void ld_span(const uint32_t *base, size_t N, size_t s, uint32_t *x) {
+  if constexpr (L0 < LE) {
+    constexpr int PW = PanelW<K, L0>::value;
+    ld_panel<PW>(base + panel_word<K, L0>(N, s), x + (L0 - X0));
+    ld_span<K, L0 + PW, LE, X0>(base, N, s, x);
+  }
+}
+
+template <int K, int L0, int LE, int X0 = L0>
+FDP_HD void st_span(uint32_t *base, size_t N, size_t s, const uint32_t *x) {
+  if constexpr (L0 < LE) {
+    constexpr int PW = PanelW<K, L0>::value;
+    st_panel<PW>(base + panel_word<K, L0>(N, s), x + (L0 - X0));
+    st_span<K, L0 + PW, LE, X0>(base, N, s, x);
+  }
+}
+
 // ---- shared-memory copies of the width tables ------------------------------
 // Heights are trimmed to FDP_HS: a legal word of at most 28 symbols never
 // rises above 14, and the kernel looks at most 2 heights above a legal one.
@@ -145,19 +179,60 @@ struct Item {
   int nc;      // closure predecessors stored in the candidate slots
 };
 
-// Decode blocked index j at cell p and hand every closure predecessor of a
-// c = N target (its main index) to on_cand.
+// A partly decoded blocked prefix: positions above `pos` are decoded (main
+// base bm, height h, high symbols hw), and j - sub is the rank left for
+// blocked positions pos..0.
+template <typename Idx>
+struct Prefix {
+  Idx sub, bm;
+  uint64_t hw;
+  int pos, h;
+};
+
+template <typename Idx>
+FDP_HD Prefix<Idx> empty_prefix(const CellArgs &a) {
+  return Prefix<Idx>{Idx(0), Idx(0), 0ull, a.W - 2, 1};
+}
+
+// The prefix shared by every blocked index in [jb, jl].  Ranks are
+// lexicographic from the top position down, so every word ranked between two
+// words carries the top symbols those two have in common: one walk of jb and
+// jl in step, stopping where they part, decodes that part for the whole range.
+template <typename Idx>
+FDP_HD Prefix<Idx> shared_prefix(const CellArgs &a, const CellSmem<Idx> &sm, const Idx jb, const Idx jl) {
+  Idx r0 = jb, r1 = jl, bm = 0;
+  int h = 1, pos = a.W - 2;
+  uint64_t hw = 0;
+  for (; pos >= a.p; --pos) {
+    const StepT<Idx> s = sm.S[pos][h];
+    const uint32_t s0 = r0 >= s.t2 ? SYM_L : (r0 >= s.t1 ? SYM_R : SYM_N);
+    const uint32_t s1 = r1 >= s.t2 ? SYM_L : (r1 >= s.t1 ? SYM_R : SYM_N);
+    if (s0 != s1) break;
+    const Idx t = s0 == SYM_L ? s.t2 : (s0 == SYM_R ? s.t1 : Idx(0));
+    r0 -= t;
+    r1 -= t;
+    bm += s0 == SYM_L ? s.cL : (s0 == SYM_R ? s.cR : Idx(0));
+    h += s0 == SYM_L ? 1 : (s0 == SYM_R ? -1 : 0);
+    hw = (hw << 2) | s0;
+  }
+  return Prefix<Idx>{Idx(jb - r0), bm, hw, pos, h};
+}
+
+// Decode blocked index j at cell p (starting from prefix pf, which j shares)
+// and hand every closure predecessor of a c = N target (its main index) to
+// on_cand.
 template <typename Idx, typename OnCand>
-FDP_HD Item<Idx> decode_item(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j, OnCand &&on_cand) {
-  const int W = a.W, p = a.p;
+FDP_HD Item<Idx> decode_item(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j, const Prefix<Idx> &pf,
+                             OnCand &&on_cand) {
+  const int p = a.p;
   Item<Idx> it;
   it.j = j;
   // Blocked prefix (blocked positions W-2..p), top-down.  hw collects the high
   // symbols so that main position q sits at bits 2*(q-p-1).
-  Idx r = j, bm = 0;
-  int h = 1;
-  uint64_t hw = 0;
-  for (int pos = W - 2; pos >= p; --pos) {
+  Idx r = j - pf.sub, bm = pf.bm;
+  int h = pf.h;
+  uint64_t hw = pf.hw;
+  for (int pos = pf.pos; pos >= p; --pos) {
     const StepT<Idx> s = sm.S[pos][h];
     const bool ge1 = r >= s.t1, ge2 = r >= s.t2;
     r -= ge2 ? s.t2 : (ge1 ? s.t1 : Idx(0));
@@ -247,114 +322,116 @@ FDP_HD Item<Idx> decode_item(const CellArgs &a, const CellSmem<Idx> &sm, const I
   return it;
 }
 
-// Several panels: the closure sources of a c = N target were staged in
-// cand[i * cstride].  Each panel is updated in the same order as the
-// one-panel path (streamed words first, closure sources last):
+// Several spans: the closure sources of a c = N target were staged in
+// cand[i * cstride].  Each span is updated in the same order as the
+// one-span path (streamed words first, closure sources last):
 //   p >= 2:  c = N: NN' = NN + B, LR' = LR + NN, B' = RL + closures
 //            c = R/L: X' = X + Y + B, B' = X   (X = NR/NL, Y = RN/LN)
 //   p == 1:  c = N: NN' = NN + B + RR closures, LR' = LR + NN
 //            c = R: NR' = NR + RN + B, RN' = RN + NR
 template <typename Idx, int K, int L0>
-FDP_HD void apply_panels_staged(const CellArgs &a, const Item<Idx> &it, const Idx *cand, int cstride) {
+FDP_HD void apply_spans_staged(const CellArgs &a, const Item<Idx> &it, const Idx *cand, int cstride) {
   if constexpr (L0 < K) {
-    constexpr int PW = PanelW<K, L0>::value;
-    uint32_t *const pm = a.main + size_t(L0) * a.mstates;  // this panel of main: [M][PW]
-    uint32_t *const pb = a.blk + size_t(L0) * a.items;     // this panel of blocked: [D][PW]
+    constexpr int LE = span_end_of(K, L0), G = LE - L0;
+    uint32_t *const Mn = a.main;
+    uint32_t *const Bk = a.blk;
+    const size_t M = a.mstates, D = a.items;
     const uint32_t *mod = a.mod + L0;
-    const size_t jj = size_t(it.j) * PW;
+    const size_t jj = size_t(it.j);
     if (it.c != 0) {
-      uint32_t x[PW], y[PW], z[PW];
-      ld_panel<PW>(pm + size_t(it.iA) * PW, x);
-      ld_panel<PW>(pm + size_t(it.iB) * PW, y);
-#pragma unroll
-      for (int i = 0; i < PW; ++i) z[i] = add_mod(x[i], y[i], mod[i]);
+      uint32_t x[G], y[G], z[G];
+      ld_span<K, L0, LE>(Mn, M, size_t(it.iA), x);
+      ld_span<K, L0, LE>(Mn, M, size_t(it.iB), y);
       if (!a.blk_in_zero) {
-        uint32_t b[PW];
-        ld_panel<PW>(pb + jj, b);
+        uint32_t b[G];
+        ld_span<K, L0, LE>(Bk, D, jj, b);
 #pragma unroll
-        for (int i = 0; i < PW; ++i) z[i] = add_mod(z[i], b[i], mod[i]);
-      }
-      st_panel<PW>(pm + size_t(it.iA) * PW, z);
-      if (a.p >= 2) {
-        st_panel<PW>(pb + jj, x);
+        for (int i = 0; i < G; ++i) z[i] = add_mod(add_mod(x[i], y[i], mod[i]), b[i], mod[i]);
       } else {
 #pragma unroll
-        for (int i = 0; i < PW; ++i) z[i] = add_mod(y[i], x[i], mod[i]);
-        st_panel<PW>(pm + size_t(it.iB) * PW, z);
+        for (int i = 0; i < G; ++i) z[i] = add_mod(x[i], y[i], mod[i]);
+      }
+      st_span<K, L0, LE>(Mn, M, size_t(it.iA), z);
+      if (a.p >= 2) {
+        st_span<K, L0, LE>(Bk, D, jj, x);
+      } else {
+#pragma unroll
+        for (int i = 0; i < G; ++i) z[i] = add_mod(y[i], x[i], mod[i]);
+        st_span<K, L0, LE>(Mn, M, size_t(it.iB), z);
         if (a.blk_out_p1) {
 #pragma unroll
-          for (int i = 0; i < PW; ++i) z[i] = 0;
-          st_panel<PW>(pb + jj, z);
+          for (int i = 0; i < G; ++i) z[i] = 0;
+          st_span<K, L0, LE>(Bk, D, jj, z);
         }
       }
     } else {
-      uint32_t x[PW], acc[PW];
-      ld_panel<PW>(pm + size_t(it.iA) * PW, x);
+      uint32_t x[G], acc[G];
+      ld_span<K, L0, LE>(Mn, M, size_t(it.iA), x);
       if (it.hasLR) {
-        uint32_t y[PW];
-        ld_panel<PW>(pm + size_t(it.iB) * PW, y);
+        uint32_t y[G];
+        ld_span<K, L0, LE>(Mn, M, size_t(it.iB), y);
 #pragma unroll
-        for (int i = 0; i < PW; ++i) y[i] = add_mod(y[i], x[i], mod[i]);
-        st_panel<PW>(pm + size_t(it.iB) * PW, y);
+        for (int i = 0; i < G; ++i) y[i] = add_mod(y[i], x[i], mod[i]);
+        st_span<K, L0, LE>(Mn, M, size_t(it.iB), y);
       }
       if (!a.blk_in_zero) {
-        uint32_t b[PW];
-        ld_panel<PW>(pb + jj, b);
+        uint32_t b[G];
+        ld_span<K, L0, LE>(Bk, D, jj, b);
 #pragma unroll
-        for (int i = 0; i < PW; ++i) x[i] = add_mod(x[i], b[i], mod[i]);
+        for (int i = 0; i < G; ++i) x[i] = add_mod(x[i], b[i], mod[i]);
       }
 #pragma unroll
-      for (int i = 0; i < PW; ++i) acc[i] = 0;
+      for (int i = 0; i < G; ++i) acc[i] = 0;
       if (a.p >= 2) {
-        st_panel<PW>(pm + size_t(it.iA) * PW, x);
-        if (it.hasRL) ld_panel<PW>(pm + size_t(it.iRL) * PW, acc);
+        st_span<K, L0, LE>(Mn, M, size_t(it.iA), x);
+        if (it.hasRL) ld_span<K, L0, LE>(Mn, M, size_t(it.iRL), acc);
       }
       int k = 0;
       for (; k + 1 < it.nc; k += 2) {
-        uint32_t u[PW], v[PW];
-        ld_panel<PW>(pm + size_t(cand[k * cstride]) * PW, u);
-        ld_panel<PW>(pm + size_t(cand[(k + 1) * cstride]) * PW, v);
+        uint32_t u[G], v[G];
+        ld_span<K, L0, LE>(Mn, M, size_t(cand[k * cstride]), u);
+        ld_span<K, L0, LE>(Mn, M, size_t(cand[(k + 1) * cstride]), v);
 #pragma unroll
-        for (int i = 0; i < PW; ++i) acc[i] = add_mod(add_mod(acc[i], u[i], mod[i]), v[i], mod[i]);
+        for (int i = 0; i < G; ++i) acc[i] = add_mod(add_mod(acc[i], u[i], mod[i]), v[i], mod[i]);
       }
       if (k < it.nc) {
-        uint32_t u[PW];
-        ld_panel<PW>(pm + size_t(cand[k * cstride]) * PW, u);
+        uint32_t u[G];
+        ld_span<K, L0, LE>(Mn, M, size_t(cand[k * cstride]), u);
 #pragma unroll
-        for (int i = 0; i < PW; ++i) acc[i] = add_mod(acc[i], u[i], mod[i]);
+        for (int i = 0; i < G; ++i) acc[i] = add_mod(acc[i], u[i], mod[i]);
       }
       if (a.p >= 2) {
-        st_panel<PW>(pb + jj, acc);
+        st_span<K, L0, LE>(Bk, D, jj, acc);
       } else {
 #pragma unroll
-        for (int i = 0; i < PW; ++i) x[i] = add_mod(x[i], acc[i], mod[i]);
-        st_panel<PW>(pm + size_t(it.iA) * PW, x);
+        for (int i = 0; i < G; ++i) x[i] = add_mod(x[i], acc[i], mod[i]);
+        st_span<K, L0, LE>(Mn, M, size_t(it.iA), x);
         if (a.blk_out_p1) {
 #pragma unroll
-          for (int i = 0; i < PW; ++i) acc[i] = 0;
-          st_panel<PW>(pb + jj, acc);
+          for (int i = 0; i < G; ++i) acc[i] = 0;
+          st_span<K, L0, LE>(Bk, D, jj, acc);
         }
       }
     }
-    apply_panels_staged<Idx, K, L0 + PW>(a, it, cand, cstride);
+    apply_spans_staged<Idx, K, LE>(a, it, cand, cstride);
   }
 }
 
 // Whether the cell kernel for K lanes stages closure candidates in shared
-// memory (several panels) or sums them while decoding (one panel).
+// memory (several spans) or sums them while decoding (one span).
 template <int K>
-constexpr bool stages_candidates() { return panel_count<K>() > 1; }
+constexpr bool stages_candidates() { return span_count<K>() > 1; }
 
-// One panel (K = 1, 2, 4 or 8): decode, update the streamed words first, then
-// add the closure sources as they are found.  Branchy per item type: measured
+// One span (K <= 8): decode, update the streamed words first, then add the
+// closure sources as they are found.  Branchy per item type: measured
 // faster than a uniform path on B200 (fewer instructions, full-sector stores).
 template <typename Idx, int K>
-FDP_HD void cell_item_one_panel(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j) {
+FDP_HD void cell_item_one_span(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j, const Prefix<Idx> &pf) {
   const int W = a.W, p = a.p;
-  Idx r = j, bm = 0;
-  int h = 1;
-  uint64_t hw = 0;  // high symbols: main position q at bits 2*(q-p-1)
-  for (int pos = W - 2; pos >= p; --pos) {
+  Idx r = j - pf.sub, bm = pf.bm;
+  int h = pf.h;
+  uint64_t hw = pf.hw;  // high symbols: main position q at bits 2*(q-p-1)
+  for (int pos = pf.pos; pos >= p; --pos) {
     const StepT<Idx> s = sm.S[pos][h];
     uint32_t sym = SYM_N;
     if (r >= s.t1) {
@@ -376,6 +453,7 @@ FDP_HD void cell_item_one_panel(const CellArgs &a, const CellSmem<Idx> &sm, cons
   const Idx *off = sm.OFF[h];
   uint32_t *const Mn = a.main;
   uint32_t *const Bk = a.blk;
+  const size_t M = a.mstates, D = a.items;
   const uint32_t *mod = a.mod;
   if (c != 0) {
     // c = R: NR' = NR + RN + B, B' = NR ;  c = L: NL' = NL + LN + B, B' = NL.
@@ -383,27 +461,27 @@ FDP_HD void cell_item_one_panel(const CellArgs &a, const CellSmem<Idx> &sm, cons
     const Idx i1 = bm + off[c == 1 ? PR_NR : PR_NL] + r;
     const Idx i2 = bm + off[c == 1 ? PR_RN : PR_LN] + r;
     uint32_t x[K], y[K], z[K];
-    ld_panel<K>(Mn + size_t(i1) * K, x);
-    ld_panel<K>(Mn + size_t(i2) * K, y);
+    ld_span<K, 0, K>(Mn, M, size_t(i1), x);
+    ld_span<K, 0, K>(Mn, M, size_t(i2), y);
 #pragma unroll
     for (int i = 0; i < K; ++i) z[i] = add_mod(x[i], y[i], mod[i]);
     if (!a.blk_in_zero) {
       uint32_t b[K];
-      ld_panel<K>(Bk + size_t(j) * K, b);
+      ld_span<K, 0, K>(Bk, D, size_t(j), b);
 #pragma unroll
       for (int i = 0; i < K; ++i) z[i] = add_mod(z[i], b[i], mod[i]);
     }
-    st_panel<K>(Mn + size_t(i1) * K, z);
+    st_span<K, 0, K>(Mn, M, size_t(i1), z);
     if (p >= 2) {
-      st_panel<K>(Bk + size_t(j) * K, x);
+      st_span<K, 0, K>(Bk, D, size_t(j), x);
     } else {
 #pragma unroll
       for (int i = 0; i < K; ++i) z[i] = add_mod(y[i], x[i], mod[i]);
-      st_panel<K>(Mn + size_t(i2) * K, z);
+      st_span<K, 0, K>(Mn, M, size_t(i2), z);
       if (a.blk_out_p1) {
 #pragma unroll
         for (int i = 0; i < K; ++i) z[i] = 0;
-        st_panel<K>(Bk + size_t(j) * K, z);
+        st_span<K, 0, K>(Bk, D, size_t(j), z);
       }
     }
     return;
@@ -413,29 +491,29 @@ FDP_HD void cell_item_one_panel(const CellArgs &a, const CellSmem<Idx> &sm, cons
   const Idx iNN = bm + off[PR_NN] + r;
   const Idx iLR = bm + off[PR_LR] + r;
   uint32_t x[K], acc[K];
-  ld_panel<K>(Mn + size_t(iNN) * K, x);
+  ld_span<K, 0, K>(Mn, M, size_t(iNN), x);
   if (h + 1 <= a.cap) {  // the LR target exists below the height cap
     uint32_t y[K];
-    ld_panel<K>(Mn + size_t(iLR) * K, y);
+    ld_span<K, 0, K>(Mn, M, size_t(iLR), y);
 #pragma unroll
     for (int i = 0; i < K; ++i) y[i] = add_mod(y[i], x[i], mod[i]);
-    st_panel<K>(Mn + size_t(iLR) * K, y);
+    st_span<K, 0, K>(Mn, M, size_t(iLR), y);
   }
   if (!a.blk_in_zero) {
     uint32_t b[K];
-    ld_panel<K>(Bk + size_t(j) * K, b);
+    ld_span<K, 0, K>(Bk, D, size_t(j), b);
 #pragma unroll
     for (int i = 0; i < K; ++i) x[i] = add_mod(x[i], b[i], mod[i]);
   }
 #pragma unroll
   for (int i = 0; i < K; ++i) acc[i] = 0;
   if (p >= 2) {
-    st_panel<K>(Mn + size_t(iNN) * K, x);
-    if (h > 0) ld_panel<K>(Mn + size_t(bm + off[PR_RL] + r) * K, acc);
+    st_span<K, 0, K>(Mn, M, size_t(iNN), x);
+    if (h > 0) ld_span<K, 0, K>(Mn, M, size_t(bm + off[PR_RL] + r), acc);
   }
   auto add_source = [&](Idx idx) {
     uint32_t u[K];
-    ld_panel<K>(Mn + size_t(idx) * K, u);
+    ld_span<K, 0, K>(Mn, M, size_t(idx), u);
 #pragma unroll
     for (int i = 0; i < K; ++i) acc[i] = add_mod(acc[i], u[i], mod[i]);
   };
@@ -487,28 +565,29 @@ FDP_HD void cell_item_one_panel(const CellArgs &a, const CellSmem<Idx> &sm, cons
     }
   }
   if (p >= 2) {
-    st_panel<K>(Bk + size_t(j) * K, acc);
+    st_span<K, 0, K>(Bk, D, size_t(j), acc);
   } else {
 #pragma unroll
     for (int i = 0; i < K; ++i) x[i] = add_mod(x[i], acc[i], mod[i]);
-    st_panel<K>(Mn + size_t(iNN) * K, x);
+    st_span<K, 0, K>(Mn, M, size_t(iNN), x);
     if (a.blk_out_p1) {
 #pragma unroll
       for (int i = 0; i < K; ++i) acc[i] = 0;
-      st_panel<K>(Bk + size_t(j) * K, acc);
+      st_span<K, 0, K>(Bk, D, size_t(j), acc);
     }
   }
 }
 
 template <typename Idx, int K>
-FDP_HD void cell_item(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j, Idx *cand, int cstride) {
+FDP_HD void cell_item(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j, const Prefix<Idx> &pf, Idx *cand,
+                      int cstride) {
   if constexpr (!stages_candidates<K>()) {
     (void)cand; (void)cstride;
-    cell_item_one_panel<Idx, K>(a, sm, j);
+    cell_item_one_span<Idx, K>(a, sm, j, pf);
   } else {
     int n = 0;
-    const Item<Idx> it = decode_item<Idx>(a, sm, j, [&](Idx idx) { cand[(n++) * cstride] = idx; });
-    apply_panels_staged<Idx, K, 0>(a, it, cand, cstride);
+    const Item<Idx> it = decode_item<Idx>(a, sm, j, pf, [&](Idx idx) { cand[(n++) * cstride] = idx; });
+    apply_spans_staged<Idx, K, 0>(a, it, cand, cstride);
   }
 }
 

@@ -30,16 +30,28 @@ constexpr size_t cell_smem_bytes(int block) {
 }
 
 template <typename Idx, int K>
-__global__ void __launch_bounds__(256) cell_kernel(const CellArgs a) {
+__global__ void __launch_bounds__(256, 4) cell_kernel(const CellArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CellSmem<Idx> &sm = *reinterpret_cast<CellSmem<Idx> *>(smem_raw);
   Idx *cand = reinterpret_cast<Idx *>(smem_raw + sizeof(CellSmem<Idx>));
   load_cell_smem<Idx>(sm, reinterpret_cast<const WidthTables<Idx> *>(a.tables), a.W, a.p);
   __syncthreads();
+  // Each warp takes chunks of 32 * lane_items consecutive blocked indices;
+  // lane l handles indices l, l + 32, ... of its chunk, so every access of a
+  // warp still covers 32 consecutive states.  With share_prefix the top
+  // symbols common to the whole chunk are decoded once (a warp-uniform walk on
+  // broadcast shared-memory reads) instead of once per index.
   const Idx n = Idx(a.items);
-  const Idx stride = Idx(gridDim.x) * blockDim.x;
-  for (Idx j = Idx(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride)
-    cell_item<Idx, K>(a, sm, j, cand + threadIdx.x, int(blockDim.x));
+  const Idx chunk = Idx(32) * Idx(a.lane_items > 0 ? a.lane_items : 1);
+  const Idx wpb = Idx(blockDim.x >> 5);
+  const Idx step = Idx(gridDim.x) * wpb * chunk;
+  const Idx lane = Idx(threadIdx.x & 31);
+  for (Idx jb = (Idx(blockIdx.x) * wpb + Idx(threadIdx.x >> 5)) * chunk; jb < n; jb += step) {
+    const Idx jl = (n - jb > chunk) ? jb + chunk - 1 : n - 1;
+    const Prefix<Idx> pf = a.share_prefix ? shared_prefix<Idx>(a, sm, jb, jl) : empty_prefix<Idx>(a);
+    for (Idx j = jb + lane; j <= jl; j += 32) cell_item<Idx, K>(a, sm, j, pf, cand + threadIdx.x, int(blockDim.x));
+    if (n - jb <= step) break;  // the next chunk start would be past n (and may wrap)
+  }
 }
 
 template <typename Idx, int K>

@@ -86,6 +86,8 @@ cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_
   a.cap = t.cap;
   a.blk_in_zero = blk_in_zero ? 1 : 0;
   a.blk_out_p1 = blk_out_p1 ? 1 : 0;
+  a.lane_items = cfg.lane_items < 1 ? 1 : cfg.lane_items;
+  a.share_prefix = (t.W - 1 - p) >= cfg.share_min ? 1 : 0;
   const bool one_panel = (K == 1 || K == 2 || K == 4 || K == 8);
   if (one_panel || !cfg.split_panels) return launch_cell_k(t, K, a, cfg, s);
   // Every panel is an independent [N][PW] array: run each as its own K = PW problem.

@@ -27,6 +27,8 @@ struct LaunchCfg {
   int grid = 0;              // 0: sized from occupancy (a multiple of the SM count)
   bool split_panels = false; // several panels: one single-panel launch per panel
   bool bounded_prefix = true;  // first rows in height-bounded spaces
+  int lane_items = 8;        // items per lane of a warp chunk of the cell kernel
+  int share_min = 4;         // share the chunk's prefix decode when it walks >= this many positions
 };
 
 template <typename Idx, int K>

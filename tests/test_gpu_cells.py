@@ -95,13 +95,17 @@ def test_zero_input_stays_zero(engine):
 
 
 def test_tuning_never_changes_results(engine):
-    # block size, grid size and panel splitting are performance knobs only
+    # block size, grid size, panel splitting, warp-chunk size and prefix
+    # sharing are performance knobs only
     try:
-        for block, grid, split in ((128, 0, True), (64, 37, False), (256, 1, True), (96, 0, False)):
-            engine.set_tuning(block=block, grid=grid, split_panels=split)
+        for block, grid, split, items, share in ((128, 0, True, 1, 99), (64, 37, False, 7, 1),
+                                                  (256, 1, True, 64, 1), (96, 0, False, 3, 5),
+                                                  (256, 0, False, 1, 1)):
+            engine.set_tuning(block=block, grid=grid, split_panels=split, lane_items=items, share_min=share)
             assert engine.get_tuning() == {"block": block, "grid": grid, "split_panels": split,
-                                           "bounded_prefix": True}
+                                           "bounded_prefix": True, "lane_items": items, "share_min": share}
             _run(engine, 12, 11, 1, [MODS[i % 3] for i in range(14)], seed=block + grid)
+            _run(engine, 12, 3, 1, [MODS[i % 3] for i in range(8)], seed=block + items)
     finally:
         engine.set_tuning()
 

@@ -170,8 +170,13 @@ fdp_status fdp_time_cells(fdp_ctx *ctx, const fdp_problem *problem, int rows, do
  * kernel takes chunks of 32 * lane_items consecutive blocked states (0 = the
  * default, 8); share_min: when a cell's high prefix is at least this many
  * symbols long, the symbols a whole chunk shares are decoded once per chunk
- * (0 = the default, 4; a value above the width never shares).  Results never
- * depend on these settings.
+ * (0 = the default, 4; a value above the width never shares); compact_max_p:
+ * cells p <= compact_max_p, where the items of one warp mix centre types,
+ * decode a chunk's items first and update them grouped by type (0 = the
+ * default, 7; -1 = never); compact_items: states per lane of such a cell's
+ * chunks, 1..4 (0 = automatic: 4 when the lanes fit one span of 8, else 2,
+ * which leaves more of the SM's on-chip memory to L1).  Results never depend
+ * on these settings.
  */
 typedef struct fdp_tuning {
   int block;
@@ -180,6 +185,8 @@ typedef struct fdp_tuning {
   int bounded_prefix;  /* first rows in height-bounded spaces (default 1)       */
   int lane_items;      /* states per lane of a warp chunk, 0..64 (0: default)   */
   int share_min;       /* shortest prefix decoded once per chunk (0: default)   */
+  int compact_max_p;   /* highest cell grouped by centre type (0: default, -1: none) */
+  int compact_items;   /* states per lane of a grouped chunk, 0..4 (0: automatic) */
 } fdp_tuning;
 fdp_status fdp_set_tuning(fdp_ctx *ctx, const fdp_tuning *tuning);
 fdp_status fdp_get_tuning(fdp_ctx *ctx, fdp_tuning *tuning);

@@ -394,8 +394,10 @@ void fdp_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   if (!c || !t) return FDP_ERR_ARGS;
   if (t->block < 64 || t->block > 256 || t->block % 32 || t->grid < 0 || t->lane_items < 0 || t->lane_items > 64 ||
-      t->share_min < 0) {
-    g_last_error = "tuning: block must be a multiple of 32 in 64..256, grid >= 0, lane_items 0..64, share_min >= 0";
+      t->share_min < 0 || t->compact_max_p < -1 || t->compact_items < 0 || t->compact_items > FDP_REC_MAX_ITEMS) {
+    g_last_error =
+        "tuning: block must be a multiple of 32 in 64..256, grid >= 0, lane_items 0..64, share_min >= 0, "
+        "compact_max_p >= -1, compact_items 0..4";
     return FDP_ERR_ARGS;
   }
   std::lock_guard<std::mutex> lk(c->mu);
@@ -405,6 +407,8 @@ extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   c->cfg.bounded_prefix = t->bounded_prefix != 0;
   c->cfg.lane_items = t->lane_items > 0 ? t->lane_items : fdp::LaunchCfg{}.lane_items;
   c->cfg.share_min = t->share_min > 0 ? t->share_min : fdp::LaunchCfg{}.share_min;
+  c->cfg.compact_max_p = t->compact_max_p != 0 ? t->compact_max_p : fdp::LaunchCfg{}.compact_max_p;
+  c->cfg.compact_items = t->compact_items;
   return FDP_OK;
 }
 
@@ -417,6 +421,8 @@ extern "C" fdp_status fdp_get_tuning(fdp_ctx *c, fdp_tuning *t) {
   t->bounded_prefix = c->cfg.bounded_prefix ? 1 : 0;
   t->lane_items = c->cfg.lane_items;
   t->share_min = c->cfg.share_min;
+  t->compact_max_p = c->cfg.compact_max_p;
+  t->compact_items = c->cfg.compact_items;
   return FDP_OK;
 }
 

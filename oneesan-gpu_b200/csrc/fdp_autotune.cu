@@ -69,7 +69,10 @@ extern "C" fdp_status fdp_autotune(fdp_ctx *c, const fdp_problem *pr, uint64_t b
     const int npanels = panel_count(L);
     for (int split = 0; split <= (npanels > 1 ? 1 : 0); ++split)
       for (int block : {128, 256}) {
-        fdp_tuning t{block, 0, split, saved.bounded_prefix, saved.lane_items, saved.share_min};
+        fdp_tuning t = saved;
+        t.block = block;
+        t.grid = 0;
+        t.split_panels = split;
         fdp_status s = fdp_set_tuning(c, &t);
         std::vector<double> samples;
         for (int r = 0; r <= repeats && s == FDP_OK; ++r) {

@@ -15,19 +15,26 @@ namespace fdp {
 
 template <typename Idx, int K>
 cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t s) {
-  const size_t smem = cell_smem_bytes<Idx, K>(cfg.block);
+  const int rec_items = a.compact ? a.lane_items : 0;  // <= FDP_REC_MAX_ITEMS (launch_cell)
+  const size_t smem = cell_smem_bytes<Idx, K>(cfg.block, rec_items);
   // Per-variant state, resolved on first use (the device is the same for the
-  // life of the process in this library's contexts).
-  static int configured_block = 0, per_sm = 0;
+  // life of the process in this library's contexts): the shared-memory limit
+  // is raised to the largest record store once, and occupancy is known for
+  // every record size.
+  static int configured_block = 0, per_sm[FDP_REC_MAX_ITEMS + 1] = {};
   if (configured_block != cfg.block) {
-    cudaError_t e = cudaFuncSetAttribute(cell_kernel<Idx, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const size_t most = cell_smem_bytes<Idx, K>(cfg.block, FDP_REC_MAX_ITEMS);
+    cudaError_t e = cudaFuncSetAttribute(cell_kernel<Idx, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(most));
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cell_kernel<Idx, K>, cfg.block, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
+    for (int c = 0; c <= FDP_REC_MAX_ITEMS; ++c) {
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[c], cell_kernel<Idx, K>, cfg.block,
+                                                        cell_smem_bytes<Idx, K>(cfg.block, c));
+      if (e != cudaSuccess) return e;
+      if (per_sm[c] < 1) per_sm[c] = 1;
+    }
     configured_block = cfg.block;
   }
-  int grid = cfg.grid > 0 ? cfg.grid : device_sm_count() * per_sm;
+  int grid = cfg.grid > 0 ? cfg.grid : device_sm_count() * per_sm[rec_items];
   const uint64_t per_block = uint64_t(cfg.block) * uint64_t(a.lane_items < 1 ? 1 : a.lane_items);
   const uint64_t need = (a.items + per_block - 1) / per_block;
   if (uint64_t(grid) > need) grid = int(need ? need : 1);

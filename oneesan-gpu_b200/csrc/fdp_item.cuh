@@ -43,6 +43,7 @@ struct CellArgs {
   int cap;             // height cap of the state space (FDP_FULL_CAP: unbounded)
   int lane_items;      // items per lane of one warp chunk (the chunk is 32 * lane_items indices)
   int share_prefix;    // decode the prefix a warp chunk shares once per chunk
+  int compact;         // update a chunk's items grouped by centre type (lane_items <= FDP_REC_MAX_ITEMS)
 };
 
 struct FirstRowArgs {
@@ -131,7 +132,7 @@ FDP_HD constexpr int span_end_of(int K, int L0) {
 }
 
 template <int K>
-constexpr int span_count() {
+FDP_HD constexpr int span_count() {
   int n = 0;
   for (int l = 0; l < K; l = span_end_of(K, l)) ++n;
   return n;
@@ -167,16 +168,25 @@ struct CellSmem {
   Idx OFF[FDP_HS][PR_COUNT];
 };
 
-// The decoded work item.
+// The decoded head of a work item: blocked index j, its high prefix (main base
+// bm, end height h, high symbols hw with main position q at bits 2*(q-p-1)),
+// the centre symbol c at blocked position p-1 (0 = N, 1 = R, 2 = L) and the
+// low rank r.
 template <typename Idx>
-struct Item {
-  Idx j;       // blocked index
-  Idx iA, iB;  // owned main words: NN/LR (c=N), NR/RN (c=R), NL/LN (c=L)
-  Idx iRL;     // RL source (c = N, h > 0)
-  int c;       // centre symbol 0=N 1=R 2=L
-  int hasRL;
-  int hasLR;   // the LR target exists (always, except at the height cap)
-  int nc;      // closure predecessors stored in the candidate slots
+struct Head {
+  Idx j, r, bm;
+  uint64_t hw;
+  int h, c;
+};
+
+// A c = N item after its closure sources were staged in the candidate slots.
+template <typename Idx>
+struct NItem {
+  Idx j;
+  Idx iNN, iLR, iRL;  // owned NN and LR words, RL source
+  int hasRL;          // the RL source exists (h > 0, p >= 2)
+  int hasLR;          // the LR target exists (always, except at the height cap)
+  int nc;             // closure sources in the candidate slots
 };
 
 // A partly decoded blocked prefix: positions above `pos` are decoded (main
@@ -218,17 +228,12 @@ FDP_HD Prefix<Idx> shared_prefix(const CellArgs &a, const CellSmem<Idx> &sm, con
   return Prefix<Idx>{Idx(jb - r0), bm, hw, pos, h};
 }
 
-// Decode blocked index j at cell p (starting from prefix pf, which j shares)
-// and hand every closure predecessor of a c = N target (its main index) to
-// on_cand.
-template <typename Idx, typename OnCand>
-FDP_HD Item<Idx> decode_item(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j, const Prefix<Idx> &pf,
-                             OnCand &&on_cand) {
+// Decode blocked index j at cell p, starting from a prefix pf that j shares:
+// the rest of the high prefix (blocked positions pf.pos..p, top-down), then
+// the centre symbol and the low rank.
+template <typename Idx>
+FDP_HD Head<Idx> decode_head(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j, const Prefix<Idx> &pf) {
   const int p = a.p;
-  Item<Idx> it;
-  it.j = j;
-  // Blocked prefix (blocked positions W-2..p), top-down.  hw collects the high
-  // symbols so that main position q sits at bits 2*(q-p-1).
   Idx r = j - pf.sub, bm = pf.bm;
   int h = pf.h;
   uint64_t hw = pf.hw;
@@ -240,97 +245,137 @@ FDP_HD Item<Idx> decode_item(const CellArgs &a, const CellSmem<Idx> &sm, const I
     h += ge2 ? 1 : (ge1 ? -1 : 0);
     hw = (hw << 2) | uint64_t(ge2 ? SYM_L : (ge1 ? SYM_R : SYM_N));
   }
-  // Centre symbol at blocked position p-1 and the low rank r.
   int c = 0;
-  {
-    const Idx bN = sm.H[p - 1][h];
-    if (r >= bN) {
-      r -= bN;
-      const Idx bR = h > 0 ? sm.H[p - 1][h - 1] : Idx(0);
-      if (r < bR) c = 1;
-      else { r -= bR; c = 2; }
-    }
+  const Idx bN = sm.H[p - 1][h];
+  if (r >= bN) {
+    r -= bN;
+    const Idx bR = h > 0 ? sm.H[p - 1][h - 1] : Idx(0);
+    if (r < bR) c = 1;
+    else { r -= bR; c = 2; }
   }
-  const Idx *off = sm.OFF[h];
-  it.c = c;
-  it.iA = bm + off[c == 0 ? PR_NN : (c == 1 ? PR_NR : PR_NL)] + r;
-  it.iB = bm + off[c == 0 ? PR_LR : (c == 1 ? PR_RN : PR_LN)] + r;
-  it.hasRL = (c == 0 && h > 0 && p >= 2) ? 1 : 0;
-  it.hasLR = (c != 0 || h + 1 <= a.cap) ? 1 : 0;
-  it.iRL = bm + off[PR_RL] + r;
-  int nc = 0;
-  if (c == 0) {
-    // LL closures (p >= 3): every L at depth 1 of the low word, flipped to R,
-    // is a predecessor with pair LL (RV.hpp:49-69 enumerates the same set).
-    // Its rank from height h+2 is the +2-shifted prefix rank, plus H[pos][hb+2]
-    // for the R, plus the unchanged remainder below.
-    if (p >= 3) {
-      const Idx baseLL = bm + off[PR_LL];
-      Idx rem = r, pre2 = 0;
-      int hb = h, depth = 1, mx = h;  // mx: highest height so far (the predecessor sits 2 higher)
-      for (int pos = p - 2; pos >= 0 && depth > 0; --pos) {
-        const Idx z0 = sm.H[pos][hb];
-        if (rem < z0) continue;  // N: no contribution at either height
-        rem -= z0;
-        const Idx z1 = hb > 0 ? sm.H[pos][hb - 1] : Idx(0);
-        const Idx up2 = sm.H[pos][hb + 2];
-        if (rem < z1) {  // R
-          pre2 += up2;
-          --depth; --hb;
-        } else {         // L
-          rem -= z1;
-          if (depth == 1 && mx + 2 <= a.cap) { on_cand(baseLL + pre2 + up2 + rem); ++nc; }
-          pre2 += up2 + sm.H[pos][hb + 1];
-          ++depth; ++hb;
-          mx = hb > mx ? hb : mx;
-        }
-      }
-    }
-    // RR closures: every R at depth 1 of the high part (scanning up from
-    // p+1), flipped to L, is a predecessor with pair RR (RV.hpp:70-82).  Its
-    // high base is bm - S0 + S2 + H[q][h], S0/S2 the rank contributions of the
-    // positions below q at their own and at +2 heights.  N symbols are skipped
-    // with the non-N bit mask.
-    const Idx offRR = sm.OFF[h + 2][PR_RR] + r;
-    uint64_t nn = (hw | (hw >> 1)) & 0x5555555555555555ull;
-    Idx S0 = 0, S2 = 0;
-    int ha = h, depth = 1, mx = h;  // mx: highest height below q (the predecessor sits 2 higher)
-    while (nn && depth > 0) {
-#if defined(__CUDA_ARCH__)
-      const int b = __ffsll((long long)nn) - 1;
-#else
-      const int b = __builtin_ctzll(nn);
-#endif
-      nn &= nn - 1;
-      const int q = p + 1 + (b >> 1);
-      if (((hw >> b) & 3u) == SYM_R) {
-        const int hbq = ha + 1;
-        if (depth == 1 && mx + 2 <= a.cap) { on_cand(bm - S0 + S2 + sm.H[q][h] + offRR); ++nc; }
-        S0 += sm.H[q][hbq];
-        S2 += sm.H[q][hbq + 2];
-        ha = hbq; ++depth;
-        mx = hbq > mx ? hbq : mx;
-      } else {
-        const int hbq = ha - 1;
-        S0 += sm.H[q][hbq] + (hbq > 0 ? sm.H[q][hbq - 1] : Idx(0));
-        S2 += sm.H[q][hbq + 2] + sm.H[q][hbq + 1];
-        ha = hbq; --depth;
-      }
-    }
-  }
-  it.nc = nc;
-  return it;
+  return Head<Idx>{j, r, bm, hw, h, c};
 }
 
-// Several spans: the closure sources of a c = N target were staged in
-// cand[i * cstride].  Each span is updated in the same order as the
-// one-span path (streamed words first, closure sources last):
-//   p >= 2:  c = N: NN' = NN + B, LR' = LR + NN, B' = RL + closures
-//            c = R/L: X' = X + Y + B, B' = X   (X = NR/NL, Y = RN/LN)
-//   p == 1:  c = N: NN' = NN + B + RR closures, LR' = LR + NN
-//            c = R: NR' = NR + RN + B, RN' = RN + NR
-template <typename Idx, int K, int L0>
-FDP_HD void apply_spans_staged(const CellArgs &a, const Item<Idx> &it, const Idx *cand, int cstride) {
+// Every closure predecessor (its main index) of a c = N head, handed to
+// on_cand: LL sources scanning the low word down, then RR sources scanning the
+// high part up.
+template <typename Idx, typename OnCand>
+FDP_HD void for_each_closure(const CellArgs &a, const CellSmem<Idx> &sm, const Head<Idx> &hd, OnCand &&on_cand) {
+  const int p = a.p, h = hd.h;
+  const Idx r = hd.r, bm = hd.bm;
+  // LL closures (p >= 3): every L at depth 1 of the low word, flipped to R,
+  // is a predecessor with pair LL (RV.hpp:49-69 enumerates the same set).
+  // Its rank from height h+2 is the +2-shifted prefix rank, plus H[pos][hb+2]
+  // for the R, plus the unchanged remainder below.
+  if (p >= 3) {
+    const Idx baseLL = bm + sm.OFF[h][PR_LL];
+    Idx rem = r, pre2 = 0;
+    int hb = h, depth = 1, mx = h;  // mx: highest height so far (the predecessor sits 2 higher)
+    for (int pos = p - 2; pos >= 0 && depth > 0; --pos) {
+      const Idx z0 = sm.H[pos][hb];
+      if (rem < z0) continue;  // N: no contribution at either height
+      rem -= z0;
+      const Idx z1 = hb > 0 ? sm.H[pos][hb - 1] : Idx(0);
+      const Idx up2 = sm.H[pos][hb + 2];
+      if (rem < z1) {  // R
+        pre2 += up2;
+        --depth; --hb;
+      } else {         // L
+        rem -= z1;
+        if (depth == 1 && mx + 2 <= a.cap) on_cand(baseLL + pre2 + up2 + rem);
+        pre2 += up2 + sm.H[pos][hb + 1];
+        ++depth; ++hb;
+        mx = hb > mx ? hb : mx;
+      }
+    }
+  }
+  // RR closures: every R at depth 1 of the high part (scanning up from p+1),
+  // flipped to L, is a predecessor with pair RR (RV.hpp:70-82).  Its high base
+  // is bm - S0 + S2 + H[q][h], S0/S2 the rank contributions of the positions
+  // below q at their own and at +2 heights.  N symbols are skipped with the
+  // non-N bit mask.
+  const Idx offRR = sm.OFF[h + 2][PR_RR] + r;
+  const uint64_t hw = hd.hw;
+  uint64_t nn = (hw | (hw >> 1)) & 0x5555555555555555ull;
+  Idx S0 = 0, S2 = 0;
+  int ha = h, depth = 1, mx = h;  // mx: highest height below q (the predecessor sits 2 higher)
+  while (nn && depth > 0) {
+#if defined(__CUDA_ARCH__)
+    const int b = __ffsll((long long)nn) - 1;
+#else
+    const int b = __builtin_ctzll(nn);
+#endif
+    nn &= nn - 1;
+    const int q = p + 1 + (b >> 1);
+    if (((hw >> b) & 3u) == SYM_R) {
+      const int hbq = ha + 1;
+      if (depth == 1 && mx + 2 <= a.cap) on_cand(bm - S0 + S2 + sm.H[q][h] + offRR);
+      S0 += sm.H[q][hbq];
+      S2 += sm.H[q][hbq + 2];
+      ha = hbq; ++depth;
+      mx = hbq > mx ? hbq : mx;
+    } else {
+      const int hbq = ha - 1;
+      S0 += sm.H[q][hbq] + (hbq > 0 ? sm.H[q][hbq - 1] : Idx(0));
+      S2 += sm.H[q][hbq + 2] + sm.H[q][hbq + 1];
+      ha = hbq; --depth;
+    }
+  }
+}
+
+// c = R / L, one span at a time (X = NR/NL, Y = RN/LN):
+//   p >= 2:  X' = X + Y + B, B' = X
+//   p == 1:  (c = R only) NR' = NR + RN + B, RN' = RN + NR, B' = 0 if stored
+template <typename Idx, int K, int L0 = 0>
+FDP_HD void apply_x(const CellArgs &a, const Idx iA, const Idx iB, const Idx j) {
+  if constexpr (L0 < K) {
+    constexpr int LE = span_end_of(K, L0), G = LE - L0;
+    uint32_t *const Mn = a.main;
+    uint32_t *const Bk = a.blk;
+    const size_t M = a.mstates, D = a.items;
+    const uint32_t *mod = a.mod + L0;
+    uint32_t x[G], y[G], z[G];
+    ld_span<K, L0, LE>(Mn, M, size_t(iA), x);
+    ld_span<K, L0, LE>(Mn, M, size_t(iB), y);
+    if (!a.blk_in_zero) {
+      uint32_t b[G];
+      ld_span<K, L0, LE>(Bk, D, size_t(j), b);
+#pragma unroll
+      for (int i = 0; i < G; ++i) z[i] = add_mod(add_mod(x[i], y[i], mod[i]), b[i], mod[i]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < G; ++i) z[i] = add_mod(x[i], y[i], mod[i]);
+    }
+    st_span<K, L0, LE>(Mn, M, size_t(iA), z);
+    if (a.p >= 2) {
+      st_span<K, L0, LE>(Bk, D, size_t(j), x);
+    } else {
+#pragma unroll
+      for (int i = 0; i < G; ++i) z[i] = add_mod(y[i], x[i], mod[i]);
+      st_span<K, L0, LE>(Mn, M, size_t(iB), z);
+      if (a.blk_out_p1) {
+#pragma unroll
+        for (int i = 0; i < G; ++i) z[i] = 0;
+        st_span<K, L0, LE>(Bk, D, size_t(j), z);
+      }
+    }
+    apply_x<Idx, K, LE>(a, iA, iB, j);
+  }
+}
+
+template <typename Idx, int K>
+FDP_HD void item_x(const CellArgs &a, const CellSmem<Idx> &sm, const Head<Idx> &hd) {
+  const Idx *off = sm.OFF[hd.h];
+  apply_x<Idx, K>(a, hd.bm + off[hd.c == 1 ? PR_NR : PR_NL] + hd.r, hd.bm + off[hd.c == 1 ? PR_RN : PR_LN] + hd.r,
+                  hd.j);
+}
+
+// c = N with the closure sources staged in cand[i * cstride], one span at a
+// time (streamed words first, closure sources last):
+//   p >= 2:  NN' = NN + B, LR' = LR + NN, B' = RL + closures
+//   p == 1:  NN' = NN + B + RR closures, LR' = LR + NN, B' = 0 if stored
+template <typename Idx, int K, int L0 = 0>
+FDP_HD void apply_n(const CellArgs &a, const NItem<Idx> &it, const Idx *cand, int cstride) {
   if constexpr (L0 < K) {
     constexpr int LE = span_end_of(K, L0), G = LE - L0;
     uint32_t *const Mn = a.main;
@@ -338,161 +383,77 @@ FDP_HD void apply_spans_staged(const CellArgs &a, const Item<Idx> &it, const Idx
     const size_t M = a.mstates, D = a.items;
     const uint32_t *mod = a.mod + L0;
     const size_t jj = size_t(it.j);
-    if (it.c != 0) {
-      uint32_t x[G], y[G], z[G];
-      ld_span<K, L0, LE>(Mn, M, size_t(it.iA), x);
-      ld_span<K, L0, LE>(Mn, M, size_t(it.iB), y);
-      if (!a.blk_in_zero) {
-        uint32_t b[G];
-        ld_span<K, L0, LE>(Bk, D, jj, b);
+    uint32_t x[G], acc[G];
+    ld_span<K, L0, LE>(Mn, M, size_t(it.iNN), x);
+    if (it.hasLR) {
+      uint32_t y[G];
+      ld_span<K, L0, LE>(Mn, M, size_t(it.iLR), y);
 #pragma unroll
-        for (int i = 0; i < G; ++i) z[i] = add_mod(add_mod(x[i], y[i], mod[i]), b[i], mod[i]);
-      } else {
+      for (int i = 0; i < G; ++i) y[i] = add_mod(y[i], x[i], mod[i]);
+      st_span<K, L0, LE>(Mn, M, size_t(it.iLR), y);
+    }
+    if (!a.blk_in_zero) {
+      uint32_t b[G];
+      ld_span<K, L0, LE>(Bk, D, jj, b);
 #pragma unroll
-        for (int i = 0; i < G; ++i) z[i] = add_mod(x[i], y[i], mod[i]);
-      }
-      st_span<K, L0, LE>(Mn, M, size_t(it.iA), z);
-      if (a.p >= 2) {
-        st_span<K, L0, LE>(Bk, D, jj, x);
-      } else {
+      for (int i = 0; i < G; ++i) x[i] = add_mod(x[i], b[i], mod[i]);
+    }
 #pragma unroll
-        for (int i = 0; i < G; ++i) z[i] = add_mod(y[i], x[i], mod[i]);
-        st_span<K, L0, LE>(Mn, M, size_t(it.iB), z);
-        if (a.blk_out_p1) {
+    for (int i = 0; i < G; ++i) acc[i] = 0;
+    if (a.p >= 2) {
+      st_span<K, L0, LE>(Mn, M, size_t(it.iNN), x);
+      if (it.hasRL) ld_span<K, L0, LE>(Mn, M, size_t(it.iRL), acc);
+    }
+    int k = 0;
+    for (; k + 1 < it.nc; k += 2) {
+      uint32_t u[G], v[G];
+      ld_span<K, L0, LE>(Mn, M, size_t(cand[k * cstride]), u);
+      ld_span<K, L0, LE>(Mn, M, size_t(cand[(k + 1) * cstride]), v);
 #pragma unroll
-          for (int i = 0; i < G; ++i) z[i] = 0;
-          st_span<K, L0, LE>(Bk, D, jj, z);
-        }
-      }
+      for (int i = 0; i < G; ++i) acc[i] = add_mod(add_mod(acc[i], u[i], mod[i]), v[i], mod[i]);
+    }
+    if (k < it.nc) {
+      uint32_t u[G];
+      ld_span<K, L0, LE>(Mn, M, size_t(cand[k * cstride]), u);
+#pragma unroll
+      for (int i = 0; i < G; ++i) acc[i] = add_mod(acc[i], u[i], mod[i]);
+    }
+    if (a.p >= 2) {
+      st_span<K, L0, LE>(Bk, D, jj, acc);
     } else {
-      uint32_t x[G], acc[G];
-      ld_span<K, L0, LE>(Mn, M, size_t(it.iA), x);
-      if (it.hasLR) {
-        uint32_t y[G];
-        ld_span<K, L0, LE>(Mn, M, size_t(it.iB), y);
 #pragma unroll
-        for (int i = 0; i < G; ++i) y[i] = add_mod(y[i], x[i], mod[i]);
-        st_span<K, L0, LE>(Mn, M, size_t(it.iB), y);
-      }
-      if (!a.blk_in_zero) {
-        uint32_t b[G];
-        ld_span<K, L0, LE>(Bk, D, jj, b);
+      for (int i = 0; i < G; ++i) x[i] = add_mod(x[i], acc[i], mod[i]);
+      st_span<K, L0, LE>(Mn, M, size_t(it.iNN), x);
+      if (a.blk_out_p1) {
 #pragma unroll
-        for (int i = 0; i < G; ++i) x[i] = add_mod(x[i], b[i], mod[i]);
-      }
-#pragma unroll
-      for (int i = 0; i < G; ++i) acc[i] = 0;
-      if (a.p >= 2) {
-        st_span<K, L0, LE>(Mn, M, size_t(it.iA), x);
-        if (it.hasRL) ld_span<K, L0, LE>(Mn, M, size_t(it.iRL), acc);
-      }
-      int k = 0;
-      for (; k + 1 < it.nc; k += 2) {
-        uint32_t u[G], v[G];
-        ld_span<K, L0, LE>(Mn, M, size_t(cand[k * cstride]), u);
-        ld_span<K, L0, LE>(Mn, M, size_t(cand[(k + 1) * cstride]), v);
-#pragma unroll
-        for (int i = 0; i < G; ++i) acc[i] = add_mod(add_mod(acc[i], u[i], mod[i]), v[i], mod[i]);
-      }
-      if (k < it.nc) {
-        uint32_t u[G];
-        ld_span<K, L0, LE>(Mn, M, size_t(cand[k * cstride]), u);
-#pragma unroll
-        for (int i = 0; i < G; ++i) acc[i] = add_mod(acc[i], u[i], mod[i]);
-      }
-      if (a.p >= 2) {
+        for (int i = 0; i < G; ++i) acc[i] = 0;
         st_span<K, L0, LE>(Bk, D, jj, acc);
-      } else {
-#pragma unroll
-        for (int i = 0; i < G; ++i) x[i] = add_mod(x[i], acc[i], mod[i]);
-        st_span<K, L0, LE>(Mn, M, size_t(it.iA), x);
-        if (a.blk_out_p1) {
-#pragma unroll
-          for (int i = 0; i < G; ++i) acc[i] = 0;
-          st_span<K, L0, LE>(Bk, D, jj, acc);
-        }
       }
     }
-    apply_spans_staged<Idx, K, LE>(a, it, cand, cstride);
+    apply_n<Idx, K, LE>(a, it, cand, cstride);
   }
 }
 
 // Whether the cell kernel for K lanes stages closure candidates in shared
-// memory (several spans) or sums them while decoding (one span).
+// memory (several spans) or sums them while scanning (one span).
 template <int K>
-constexpr bool stages_candidates() { return span_count<K>() > 1; }
+FDP_HD constexpr bool stages_candidates() { return span_count<K>() > 1; }
 
-// One span (K <= 8): decode, update the streamed words first, then add the
-// closure sources as they are found.  Branchy per item type: measured
-// faster than a uniform path on B200 (fewer instructions, full-sector stores).
+// c = N, one span (K <= 8): update the streamed words first, then add the
+// closure sources as the scans find them (same formulas as apply_n).
 template <typename Idx, int K>
-FDP_HD void cell_item_one_span(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j, const Prefix<Idx> &pf) {
-  const int W = a.W, p = a.p;
-  Idx r = j - pf.sub, bm = pf.bm;
-  int h = pf.h;
-  uint64_t hw = pf.hw;  // high symbols: main position q at bits 2*(q-p-1)
-  for (int pos = pf.pos; pos >= p; --pos) {
-    const StepT<Idx> s = sm.S[pos][h];
-    uint32_t sym = SYM_N;
-    if (r >= s.t1) {
-      if (r >= s.t2) { r -= s.t2; bm += s.cL; ++h; sym = SYM_L; }
-      else { r -= s.t1; bm += s.cR; --h; sym = SYM_R; }
-    }
-    hw = (hw << 2) | sym;
-  }
-  int c = 0;
-  {
-    const Idx bN = sm.H[p - 1][h];
-    if (r >= bN) {
-      r -= bN;
-      const Idx bR = h > 0 ? sm.H[p - 1][h - 1] : Idx(0);
-      if (r < bR) c = 1;
-      else { r -= bR; c = 2; }
-    }
-  }
-  const Idx *off = sm.OFF[h];
+FDP_HD void item_n_one_span(const CellArgs &a, const CellSmem<Idx> &sm, const Head<Idx> &hd) {
+  const int p = a.p;
   uint32_t *const Mn = a.main;
   uint32_t *const Bk = a.blk;
   const size_t M = a.mstates, D = a.items;
   const uint32_t *mod = a.mod;
-  if (c != 0) {
-    // c = R: NR' = NR + RN + B, B' = NR ;  c = L: NL' = NL + LN + B, B' = NL.
-    // At p = 1 (only c = R reaches here): RN' = RN + NR as well.
-    const Idx i1 = bm + off[c == 1 ? PR_NR : PR_NL] + r;
-    const Idx i2 = bm + off[c == 1 ? PR_RN : PR_LN] + r;
-    uint32_t x[K], y[K], z[K];
-    ld_span<K, 0, K>(Mn, M, size_t(i1), x);
-    ld_span<K, 0, K>(Mn, M, size_t(i2), y);
-#pragma unroll
-    for (int i = 0; i < K; ++i) z[i] = add_mod(x[i], y[i], mod[i]);
-    if (!a.blk_in_zero) {
-      uint32_t b[K];
-      ld_span<K, 0, K>(Bk, D, size_t(j), b);
-#pragma unroll
-      for (int i = 0; i < K; ++i) z[i] = add_mod(z[i], b[i], mod[i]);
-    }
-    st_span<K, 0, K>(Mn, M, size_t(i1), z);
-    if (p >= 2) {
-      st_span<K, 0, K>(Bk, D, size_t(j), x);
-    } else {
-#pragma unroll
-      for (int i = 0; i < K; ++i) z[i] = add_mod(y[i], x[i], mod[i]);
-      st_span<K, 0, K>(Mn, M, size_t(i2), z);
-      if (a.blk_out_p1) {
-#pragma unroll
-        for (int i = 0; i < K; ++i) z[i] = 0;
-        st_span<K, 0, K>(Bk, D, size_t(j), z);
-      }
-    }
-    return;
-  }
-  // c = N: NN' = NN + B, LR' = LR + NN, B' = RL + closures (p >= 2);
-  //        at p = 1: NN' = NN + B + RR closures, LR' = LR + NN.
-  const Idx iNN = bm + off[PR_NN] + r;
-  const Idx iLR = bm + off[PR_LR] + r;
+  const Idx *off = sm.OFF[hd.h];
+  const Idx iNN = hd.bm + off[PR_NN] + hd.r;
+  const Idx iLR = hd.bm + off[PR_LR] + hd.r;
   uint32_t x[K], acc[K];
   ld_span<K, 0, K>(Mn, M, size_t(iNN), x);
-  if (h + 1 <= a.cap) {  // the LR target exists below the height cap
+  if (hd.h + 1 <= a.cap) {  // the LR target exists below the height cap
     uint32_t y[K];
     ld_span<K, 0, K>(Mn, M, size_t(iLR), y);
 #pragma unroll
@@ -501,7 +462,7 @@ FDP_HD void cell_item_one_span(const CellArgs &a, const CellSmem<Idx> &sm, const
   }
   if (!a.blk_in_zero) {
     uint32_t b[K];
-    ld_span<K, 0, K>(Bk, D, size_t(j), b);
+    ld_span<K, 0, K>(Bk, D, size_t(hd.j), b);
 #pragma unroll
     for (int i = 0; i < K; ++i) x[i] = add_mod(x[i], b[i], mod[i]);
   }
@@ -509,63 +470,16 @@ FDP_HD void cell_item_one_span(const CellArgs &a, const CellSmem<Idx> &sm, const
   for (int i = 0; i < K; ++i) acc[i] = 0;
   if (p >= 2) {
     st_span<K, 0, K>(Mn, M, size_t(iNN), x);
-    if (h > 0) ld_span<K, 0, K>(Mn, M, size_t(bm + off[PR_RL] + r), acc);
+    if (hd.h > 0) ld_span<K, 0, K>(Mn, M, size_t(hd.bm + off[PR_RL] + hd.r), acc);
   }
-  auto add_source = [&](Idx idx) {
+  for_each_closure<Idx>(a, sm, hd, [&](Idx idx) {
     uint32_t u[K];
     ld_span<K, 0, K>(Mn, M, size_t(idx), u);
 #pragma unroll
     for (int i = 0; i < K; ++i) acc[i] = add_mod(acc[i], u[i], mod[i]);
-  };
-  // LL closures (p >= 3): every L at depth 1 of the low word, flipped to R.
-  if (p >= 3) {
-    const Idx baseLL = bm + off[PR_LL];
-    Idx rem = r, pre2 = 0;
-    int hb = h, depth = 1, mx = h;
-    for (int pos = p - 2; pos >= 0 && depth > 0; --pos) {
-      const Idx z0 = sm.H[pos][hb];
-      if (rem < z0) continue;
-      rem -= z0;
-      const Idx z1 = hb > 0 ? sm.H[pos][hb - 1] : Idx(0);
-      const Idx up2 = sm.H[pos][hb + 2];
-      if (rem < z1) {
-        pre2 += up2;
-        --depth; --hb;
-      } else {
-        rem -= z1;
-        if (depth == 1 && mx + 2 <= a.cap) add_source(baseLL + pre2 + up2 + rem);
-        pre2 += up2 + sm.H[pos][hb + 1];
-        ++depth; ++hb;
-        mx = hb > mx ? hb : mx;
-      }
-    }
-  }
-  // RR closures: every R at depth 1 of the high part, flipped to L.
-  {
-    Idx S0 = 0, S2 = 0;
-    int ha = h, depth = 1, mx = h;
-    const Idx offRR = sm.OFF[h + 2][PR_RR] + r;
-    uint64_t w = hw;
-    for (int q = p + 1; q <= W - 1 && depth > 0; ++q, w >>= 2) {
-      const uint32_t sy = uint32_t(w) & 3u;
-      if (sy == SYM_N) continue;
-      if (sy == SYM_R) {
-        const int hbq = ha + 1;
-        if (depth == 1 && mx + 2 <= a.cap) add_source(bm - S0 + S2 + sm.H[q][h] + offRR);
-        S0 += sm.H[q][hbq];
-        S2 += sm.H[q][hbq + 2];
-        ha = hbq; ++depth;
-        mx = hbq > mx ? hbq : mx;
-      } else {
-        const int hbq = ha - 1;
-        S0 += sm.H[q][hbq] + (hbq > 0 ? sm.H[q][hbq - 1] : Idx(0));
-        S2 += sm.H[q][hbq + 2] + sm.H[q][hbq + 1];
-        ha = hbq; --depth;
-      }
-    }
-  }
+  });
   if (p >= 2) {
-    st_span<K, 0, K>(Bk, D, size_t(j), acc);
+    st_span<K, 0, K>(Bk, D, size_t(hd.j), acc);
   } else {
 #pragma unroll
     for (int i = 0; i < K; ++i) x[i] = add_mod(x[i], acc[i], mod[i]);
@@ -573,22 +487,70 @@ FDP_HD void cell_item_one_span(const CellArgs &a, const CellSmem<Idx> &sm, const
     if (a.blk_out_p1) {
 #pragma unroll
       for (int i = 0; i < K; ++i) acc[i] = 0;
-      st_span<K, 0, K>(Bk, D, size_t(j), acc);
+      st_span<K, 0, K>(Bk, D, size_t(hd.j), acc);
     }
   }
 }
 
 template <typename Idx, int K>
-FDP_HD void cell_item(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j, const Prefix<Idx> &pf, Idx *cand,
-                      int cstride) {
+FDP_HD void item_n(const CellArgs &a, const CellSmem<Idx> &sm, const Head<Idx> &hd, Idx *cand, int cstride) {
   if constexpr (!stages_candidates<K>()) {
     (void)cand; (void)cstride;
-    cell_item_one_span<Idx, K>(a, sm, j, pf);
+    item_n_one_span<Idx, K>(a, sm, hd);
   } else {
+    const Idx *off = sm.OFF[hd.h];
+    NItem<Idx> it;
+    it.j = hd.j;
+    it.iNN = hd.bm + off[PR_NN] + hd.r;
+    it.iLR = hd.bm + off[PR_LR] + hd.r;
+    it.iRL = hd.bm + off[PR_RL] + hd.r;
+    it.hasRL = (hd.h > 0 && a.p >= 2) ? 1 : 0;
+    it.hasLR = (hd.h + 1 <= a.cap) ? 1 : 0;
     int n = 0;
-    const Item<Idx> it = decode_item<Idx>(a, sm, j, pf, [&](Idx idx) { cand[(n++) * cstride] = idx; });
-    apply_spans_staged<Idx, K, 0>(a, it, cand, cstride);
+    for_each_closure<Idx>(a, sm, hd, [&](Idx idx) { cand[(n++) * cstride] = idx; });
+    it.nc = n;
+    apply_n<Idx, K>(a, it, cand, cstride);
   }
+}
+
+// Decoded heads of one warp chunk in shared memory (structure of arrays of
+// `cap` entries): the compacted kernel path stores every head of a chunk
+// first, then updates the c = R/L items and the c = N items each with whole
+// warps.
+#define FDP_REC_MAX_ITEMS 4  // states per lane of a compacted chunk, at most
+template <typename Idx>
+FDP_HD constexpr size_t head_rec_entry_bytes() {
+  return sizeof(uint64_t) + 3 * sizeof(Idx) + sizeof(uint32_t);
+}
+
+template <typename Idx>
+struct HeadRecs {
+  unsigned char *base;  // hw[cap] (u64), then j[cap], r[cap], bm[cap] (Idx), then hc[cap] = h | c << 8
+  int cap;
+  FDP_HD uint64_t *hw() const { return reinterpret_cast<uint64_t *>(base); }
+  FDP_HD Idx *idx(int field) const { return reinterpret_cast<Idx *>(base + size_t(cap) * 8) + field * cap; }
+  FDP_HD uint32_t *hc() const { return reinterpret_cast<uint32_t *>(base + size_t(cap) * (8 + 3 * sizeof(Idx))); }
+  FDP_HD void put(int k, const Head<Idx> &h) const {
+    hw()[k] = h.hw;
+    idx(0)[k] = h.j;
+    idx(1)[k] = h.r;
+    idx(2)[k] = h.bm;
+    hc()[k] = uint32_t(h.h) | (uint32_t(h.c) << 8);
+  }
+  FDP_HD Head<Idx> get(int k) const {
+    const uint32_t v = hc()[k];
+    return Head<Idx>{idx(0)[k], idx(1)[k], idx(2)[k], hw()[k], int(v & 255u), int(v >> 8)};
+  }
+};
+
+// One work item: decode blocked index j (which shares prefix pf) and update
+// the words it owns.
+template <typename Idx, int K>
+FDP_HD void cell_item(const CellArgs &a, const CellSmem<Idx> &sm, const Idx j, const Prefix<Idx> &pf, Idx *cand,
+                      int cstride) {
+  const Head<Idx> hd = decode_head<Idx>(a, sm, j, pf);
+  if (hd.c != 0) item_x<Idx, K>(a, sm, hd);
+  else item_n<Idx, K>(a, sm, hd, cand, cstride);
 }
 
 // ---- first row ----------------------------------------------------------------

@@ -22,11 +22,19 @@ __device__ __forceinline__ void load_cell_smem(CellSmem<Idx> &sm, const WidthTab
   for (int i = tid; i < FDP_HS * PR_COUNT; i += nthr) sm.OFF[i / PR_COUNT][i % PR_COUNT] = t->OFF[p][i / PR_COUNT][i % PR_COUNT];
 }
 
-// Dynamic shared memory of the cell kernel: the width tables, then the
-// closure-candidate slots (slot i of thread t at cand[i * blockDim + t]).
+// Dynamic shared memory of the cell kernel: the width tables, the
+// closure-candidate slots (slot i of thread t at cand[i * blockDim + t]), then
+// (compacted launches) one head-record store per warp.
 template <typename Idx, int K>
-constexpr size_t cell_smem_bytes(int block) {
-  return sizeof(CellSmem<Idx>) + (stages_candidates<K>() ? size_t(FDP_MAX_CAND) * block * sizeof(Idx) : 0);
+FDP_HD constexpr size_t cell_recs_offset(int block) {
+  return (sizeof(CellSmem<Idx>) + (stages_candidates<K>() ? size_t(FDP_MAX_CAND) * block * sizeof(Idx) : 0) + 15) &
+         ~size_t(15);
+}
+
+// rec_items: states per lane of a compacted chunk (0: not compacted).
+template <typename Idx, int K>
+FDP_HD constexpr size_t cell_smem_bytes(int block, int rec_items) {
+  return cell_recs_offset<Idx, K>(block) + size_t(block / 32) * size_t(32 * rec_items) * head_rec_entry_bytes<Idx>();
 }
 
 template <typename Idx, int K>
@@ -46,10 +54,43 @@ __global__ void __launch_bounds__(256, 4) cell_kernel(const CellArgs a) {
   const Idx wpb = Idx(blockDim.x >> 5);
   const Idx step = Idx(gridDim.x) * wpb * chunk;
   const Idx lane = Idx(threadIdx.x & 31);
+  // Compacted (cells where a warp's items mix centre types, p small): the
+  // heads of a chunk are decoded first and stored split by type, c = R/L from
+  // the front and c = N from the back, so each update runs on whole warps
+  // instead of two half-empty branches.  Any order of items within a cell is
+  // valid: no item reads or writes a word another item writes.
+  const bool compact = a.compact && a.lane_items <= FDP_REC_MAX_ITEMS;
+  const HeadRecs<Idx> rec{smem_raw + cell_recs_offset<Idx, K>(blockDim.x) +
+                              size_t(threadIdx.x >> 5) * size_t(chunk) * head_rec_entry_bytes<Idx>(),
+                          int(chunk)};
+  const unsigned below = (1u << (threadIdx.x & 31)) - 1u;
   for (Idx jb = (Idx(blockIdx.x) * wpb + Idx(threadIdx.x >> 5)) * chunk; jb < n; jb += step) {
     const Idx jl = (n - jb > chunk) ? jb + chunk - 1 : n - 1;
     const Prefix<Idx> pf = a.share_prefix ? shared_prefix<Idx>(a, sm, jb, jl) : empty_prefix<Idx>(a);
-    for (Idx j = jb + lane; j <= jl; j += 32) cell_item<Idx, K>(a, sm, j, pf, cand + threadIdx.x, int(blockDim.x));
+    if (!compact) {
+      for (Idx j = jb + lane; j <= jl; j += 32) cell_item<Idx, K>(a, sm, j, pf, cand + threadIdx.x, int(blockDim.x));
+    } else {
+      const int last = int(chunk) - 1;
+      const Idx span = jl - jb;
+      int nx = 0, nn = 0;
+      for (int i = 0; i < a.lane_items; ++i) {
+        const Idx o = lane + Idx(32 * i);
+        const bool valid = o <= span;
+        Head<Idx> hd{};
+        if (valid) hd = decode_head<Idx>(a, sm, jb + o, pf);
+        const bool isx = valid && hd.c != 0, isn = valid && hd.c == 0;
+        const unsigned bx = __ballot_sync(0xffffffffu, isx), bn = __ballot_sync(0xffffffffu, isn);
+        if (isx) rec.put(nx + __popc(bx & below), hd);
+        if (isn) rec.put(last - (nn + __popc(bn & below)), hd);
+        nx += __popc(bx);
+        nn += __popc(bn);
+      }
+      __syncwarp();
+      for (int k = int(lane); k < nx; k += 32) item_x<Idx, K>(a, sm, rec.get(k));
+      for (int k = int(lane); k < nn; k += 32)
+        item_n<Idx, K>(a, sm, rec.get(last - k), cand + threadIdx.x, int(blockDim.x));
+      __syncwarp();
+    }
     if (n - jb <= step) break;  // the next chunk start would be past n (and may wrap)
   }
 }

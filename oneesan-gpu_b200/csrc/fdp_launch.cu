@@ -88,6 +88,14 @@ cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_
   a.blk_out_p1 = blk_out_p1 ? 1 : 0;
   a.lane_items = cfg.lane_items < 1 ? 1 : cfg.lane_items;
   a.share_prefix = (t.W - 1 - p) >= cfg.share_min ? 1 : 0;
+  a.compact = p <= cfg.compact_max_p ? 1 : 0;
+  if (a.compact) {
+    int spans = 0;
+    for (int l = 0; l < K; l = span_end_of(K, l)) ++spans;
+    int most = cfg.compact_items > 0 ? cfg.compact_items : (spans > 1 ? 2 : 4);
+    if (most > FDP_REC_MAX_ITEMS) most = FDP_REC_MAX_ITEMS;
+    if (a.lane_items > most) a.lane_items = most;
+  }
   const bool one_panel = (K == 1 || K == 2 || K == 4 || K == 8);
   if (one_panel || !cfg.split_panels) return launch_cell_k(t, K, a, cfg, s);
   // Every panel is an independent [N][PW] array: run each as its own K = PW problem.

@@ -29,6 +29,9 @@ struct LaunchCfg {
   bool bounded_prefix = true;  // first rows in height-bounded spaces
   int lane_items = 8;        // items per lane of a warp chunk of the cell kernel
   int share_min = 4;         // share the chunk's prefix decode when it walks >= this many positions
+  int compact_max_p = 7;     // cells p <= this update a chunk's items grouped by centre type (-1: never)
+  int compact_items = 0;     // states per lane of a compacted chunk (1..FDP_REC_MAX_ITEMS; 0: 4 for
+                             // one span, 2 when closure sources are staged, which leaves L1 room)
 };
 
 template <typename Idx, int K>

@@ -98,12 +98,14 @@ def test_tuning_never_changes_results(engine):
     # block size, grid size, panel splitting, warp-chunk size and prefix
     # sharing are performance knobs only
     try:
-        for block, grid, split, items, share in ((128, 0, True, 1, 99), (64, 37, False, 7, 1),
-                                                  (256, 1, True, 64, 1), (96, 0, False, 3, 5),
-                                                  (256, 0, False, 1, 1)):
-            engine.set_tuning(block=block, grid=grid, split_panels=split, lane_items=items, share_min=share)
+        for block, grid, split, items, share, compact, citems in (
+                (128, 0, True, 1, 99, -1, 4), (64, 37, False, 7, 1, 30, 3), (256, 1, True, 64, 1, 5, 1),
+                (96, 0, False, 3, 5, 1, 2), (256, 0, False, 1, 1, 30, 4), (160, 3, False, 4, 2, 30, 4)):
+            engine.set_tuning(block=block, grid=grid, split_panels=split, lane_items=items, share_min=share,
+                              compact_max_p=compact, compact_items=citems)
             assert engine.get_tuning() == {"block": block, "grid": grid, "split_panels": split,
-                                           "bounded_prefix": True, "lane_items": items, "share_min": share}
+                                           "bounded_prefix": True, "lane_items": items, "share_min": share,
+                                           "compact_max_p": compact, "compact_items": citems}
             _run(engine, 12, 11, 1, [MODS[i % 3] for i in range(14)], seed=block + grid)
             _run(engine, 12, 3, 1, [MODS[i % 3] for i in range(8)], seed=block + items)
     finally:

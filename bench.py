@@ -79,6 +79,30 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
+# Residues the reference publishes for its GPU solvers (n, modulus) -> residue.
+PUBLISHED = {
+    (22, 4294967291): 1245069298,  # docs/results/groupbatch-interleaved-2026-09-05.json:1027
+    (21, 4294967291): 998035516,   # docs/b300-hbm32.md:554
+    (21, 4294966997): 2124618149,  # scripts/run/autotune.py:28
+    (20, 4294967291): 2308006916,  # scripts/test/groupbatch-scratch.py:17
+    (20, 4294966997): 3704549185,
+    (18, 4294967291): 503411004,   # docs/results/reverse-algorithm-2026-09-05.md:53
+}
+
+
+def published_check(n: int, moduli, residues) -> dict:
+    """Compare the residues with every published value for this n; a mismatch
+    ends the run (a wrong count has no throughput)."""
+    checked = []
+    for m, r in zip(moduli, residues):
+        want = PUBLISHED.get((n, m))
+        if want is not None:
+            if r != want:
+                raise SystemExit(f"n={n} mod {m}: residue {r} != published {want}")
+            checked.append({"modulus": m, "residue": r})
+    return {"published_residues_matched": checked}
+
+
 def committed_traffic(n: int, lanes: int):
     """Per-launch DRAM bytes of the cell kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "cell_kernel_traffic.txt")
@@ -304,6 +328,7 @@ def run_ours(args) -> None:
                    "parallelism": f"replicas x{world}"},
         "transitions_per_s": transitions / dev_s,
         "residues": results,
+        "check": published_check(n, moduli, results),
         "e2e": {"value": e2e, "unit": "residues/hour", "h2d_bytes_per_step": 4 * k,
                 "d2h_bytes_per_step": 4 * k},
         "gpu_launches": launches,

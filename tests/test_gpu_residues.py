@@ -18,6 +18,7 @@ KNOWN = [
     (18, 2147483647, 624312750),
     (20, 4294967291, 2308006916), (20, 4294966997, 3704549185),  # scripts/test/groupbatch-scratch.py:17
     (21, 4294966997, 2124618149), (21, 4294967291, 998035516),   # scripts/run/autotune.py:28, docs/b300-hbm32.md:554
+    (22, 4294967291, 1245069298),  # docs/results/groupbatch-interleaved-2026-09-05.json:1027, 1291
 ]
 
 

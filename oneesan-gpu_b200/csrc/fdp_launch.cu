@@ -169,32 +169,78 @@ struct CapTable {
   unsigned long long H[FDP_MAXW + 1][FDP_HT];
 };
 
-// dst[rank_to(w_i) * pw + l] = tmp[(i - lo) * pw + l] for the words w_i of the
-// `from` space with index i in [lo, hi).
-__global__ void expand_scatter_kernel(const CapTable *from, const CapTable *to, int W, uint64_t lo, uint64_t hi,
-                                      int pw, const uint32_t *tmp, uint32_t *dst) {
+// One step of the walk that unranks a word in the `from` space and ranks it
+// in the `to` space at once: symbol at `pos` from the residual rank r at
+// height h, its `to` rank contribution added to j.
+__device__ __forceinline__ void expand_step(const unsigned long long (*sf)[FDP_HT],
+                                            const unsigned long long (*st)[FDP_HT], int pos, uint64_t &r,
+                                            uint64_t &j, int &h) {
+  const uint64_t zN = sf[pos][h];
+  if (r < zN) return;  // N: no contribution in either space
+  r -= zN;
+  const uint64_t zR = h > 0 ? sf[pos][h - 1] : 0ull;
+  if (r < zR) {  // R
+    j += st[pos][h];
+    --h;
+    return;
+  }
+  r -= zR;  // L
+  j += st[pos][h] + (h > 0 ? st[pos][h - 1] : 0ull);
+  ++h;
+}
+
+// dst[rank_to(w_i) * PW + l] = tmp[(i - lo) * PW + l] for the words w_i of the
+// `from` space with index i in [lo, hi).  Each warp takes chunks of 32 x 8
+// consecutive indices; the top symbols the chunk's first and last words share
+// are decoded once (ranks are lexicographic from the top), each lane walks the
+// rest, and panels move as whole vectors.
+template <int PW>
+__global__ void __launch_bounds__(256) expand_scatter_kernel(const CapTable *from, const CapTable *to, int W,
+                                                             uint64_t lo, uint64_t hi, const uint32_t *tmp,
+                                                             uint32_t *dst) {
   __shared__ unsigned long long sf[FDP_MAXW + 1][FDP_HT], st[FDP_MAXW + 1][FDP_HT];
   for (int i = threadIdx.x; i < (FDP_MAXW + 1) * FDP_HT; i += blockDim.x) {
     (&sf[0][0])[i] = (&from->H[0][0])[i];
     (&st[0][0])[i] = (&to->H[0][0])[i];
   }
   __syncthreads();
-  for (uint64_t i = lo + uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < hi; i += uint64_t(gridDim.x) * blockDim.x) {
-    unsigned long long r = i;
-    uint64_t m = 0;
-    int h = 1;
-    for (int pos = W - 1; pos >= 0; --pos) {  // unrank in the `from` space
-      unsigned long long z = sf[pos][h];
-      if (r < z) continue;
-      r -= z;
-      z = h > 0 ? sf[pos][h - 1] : 0ull;
-      if (r < z) { m |= uint64_t(SYM_R) << (2 * pos); --h; continue; }
-      r -= z;
-      m |= uint64_t(SYM_L) << (2 * pos);
-      ++h;
+  constexpr uint64_t kChunk = 32 * 8;
+  const uint64_t n = hi - lo, wpb = blockDim.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t step = uint64_t(gridDim.x) * wpb * kChunk;
+  for (uint64_t cb = (uint64_t(blockIdx.x) * wpb + (threadIdx.x >> 5)) * kChunk; cb < n; cb += step) {
+    const uint64_t ce = n - cb > kChunk ? cb + kChunk : n;  // chunk [cb, ce) of [0, n)
+    uint64_t r0 = lo + cb, r1 = lo + ce - 1, j0 = 0;
+    int h = 1, pos = W - 1;
+    for (; pos >= 0; --pos) {  // the shared top symbols (warp-uniform)
+      uint64_t a0 = r0, a1 = r1, jj = j0, b1 = 0;
+      int h0 = h, h1 = h;
+      expand_step(sf, st, pos, a0, jj, h0);
+      expand_step(sf, st, pos, a1, b1, h1);
+      if (h0 != h1) break;  // the symbols differ (N keeps h, R lowers it, L raises it)
+      r0 = a0;
+      r1 = a1;
+      j0 = jj;
+      h = h0;
     }
-    const unsigned long long j = rank_dev<unsigned long long>(m, W, st);
-    for (int l = 0; l < pw; ++l) dst[size_t(j) * pw + l] = tmp[size_t(i - lo) * pw + l];
+    const uint64_t sub = lo + cb - r0;  // rank consumed by the shared symbols
+    for (uint64_t i = cb + lane; i < ce; i += 32) {
+      uint64_t r = lo + i - sub, j = j0;
+      int hh = h;
+      for (int q = pos; q >= 0; --q) expand_step(sf, st, q, r, j, hh);
+      const uint32_t *s = tmp + size_t(i) * PW;
+      uint32_t *d = dst + size_t(j) * PW;
+      if constexpr (PW == 8) {
+        reinterpret_cast<uint4 *>(d)[0] = reinterpret_cast<const uint4 *>(s)[0];
+        reinterpret_cast<uint4 *>(d)[1] = reinterpret_cast<const uint4 *>(s)[1];
+      } else if constexpr (PW == 4) {
+        *reinterpret_cast<uint4 *>(d) = *reinterpret_cast<const uint4 *>(s);
+      } else if constexpr (PW == 2) {
+        *reinterpret_cast<uint2 *>(d) = *reinterpret_cast<const uint2 *>(s);
+      } else {
+        *d = *s;
+      }
+    }
+    if (n - cb <= step) break;
   }
 }
 
@@ -251,7 +297,11 @@ cudaError_t enqueue_expand(const DevTables &from, const DevTables &to, int K, ui
       if ((e = cudaMemsetAsync(dst + size_t(nlo) * pw, 0, size_t(top - nlo) * pw * 4, s)) != cudaSuccess) return e;
       const uint64_t n = hi - lo;
       uint64_t g = (n + 255) / 256, gc = uint64_t(device_sm_count()) * 8;
-      expand_scatter_kernel<<<unsigned(g < gc ? g : gc), 256, 0, s>>>(tf, tt, W, lo, hi, pw, tmp, dst);
+      const unsigned grid = unsigned(g < gc ? g : gc);
+      if (pw == 8) expand_scatter_kernel<8><<<grid, 256, 0, s>>>(tf, tt, W, lo, hi, tmp, dst);
+      else if (pw == 4) expand_scatter_kernel<4><<<grid, 256, 0, s>>>(tf, tt, W, lo, hi, tmp, dst);
+      else if (pw == 2) expand_scatter_kernel<2><<<grid, 256, 0, s>>>(tf, tt, W, lo, hi, tmp, dst);
+      else expand_scatter_kernel<1><<<grid, 256, 0, s>>>(tf, tt, W, lo, hi, tmp, dst);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       if (launches) ++*launches;
       top = nlo;

@@ -74,4 +74,25 @@ FDP_HD uint32_t add_mod(uint32_t a, uint32_t b, uint32_t p) {
   return (s < a || s >= p) ? s - p : s;
 }
 
+// One step of a walk that unranks a main word in one state space (count table
+// F) and ranks it in another (count table T) at the same time: the symbol at
+// `pos` follows from the residual rank r at height h (N below F[pos][h], then
+// R, then L), and its rank contribution in T is added to j.  Used to move a
+// state vector between height-bounded spaces.
+template <typename T>
+FDP_HD void expand_step(const T (*F)[FDP_HT], const T (*Tt)[FDP_HT], int pos, uint64_t &r, uint64_t &j, int &h) {
+  const uint64_t zN = F[pos][h];
+  if (r < zN) return;  // N: no contribution in either space
+  r -= zN;
+  const uint64_t zR = h > 0 ? uint64_t(F[pos][h - 1]) : 0ull;
+  if (r < zR) {  // R
+    j += Tt[pos][h];
+    --h;
+    return;
+  }
+  r -= zR;  // L
+  j += uint64_t(Tt[pos][h]) + (h > 0 ? uint64_t(Tt[pos][h - 1]) : 0ull);
+  ++h;
+}
+
 }  // namespace fdp

@@ -169,26 +169,6 @@ struct CapTable {
   unsigned long long H[FDP_MAXW + 1][FDP_HT];
 };
 
-// One step of the walk that unranks a word in the `from` space and ranks it
-// in the `to` space at once: symbol at `pos` from the residual rank r at
-// height h, its `to` rank contribution added to j.
-__device__ __forceinline__ void expand_step(const unsigned long long (*sf)[FDP_HT],
-                                            const unsigned long long (*st)[FDP_HT], int pos, uint64_t &r,
-                                            uint64_t &j, int &h) {
-  const uint64_t zN = sf[pos][h];
-  if (r < zN) return;  // N: no contribution in either space
-  r -= zN;
-  const uint64_t zR = h > 0 ? sf[pos][h - 1] : 0ull;
-  if (r < zR) {  // R
-    j += st[pos][h];
-    --h;
-    return;
-  }
-  r -= zR;  // L
-  j += st[pos][h] + (h > 0 ? st[pos][h - 1] : 0ull);
-  ++h;
-}
-
 // dst[rank_to(w_i) * PW + l] = tmp[(i - lo) * PW + l] for the words w_i of the
 // `from` space with index i in [lo, hi).  Each warp takes chunks of 32 x 8
 // consecutive indices; the top symbols the chunk's first and last words share

@@ -294,6 +294,28 @@ fdp_status fdp_reverse2_apply(fdp_ctx *ctx, int width, int p, int lanes, const u
                               const uint32_t *d_in_main, const uint32_t *d_in_block, uint32_t *d_out_main,
                               uint32_t *d_out_block, void *stream);
 
+/*
+ * Residue read-out that allocates no device memory.  No counterpart in the
+ * reference, whose solver owns all device memory itself.
+ *
+ * For callers that cannot let a library call cudaMalloc: a serving process or
+ * framework whose own pool allocator already holds the GPU's memory (an
+ * allocation would fail or break the pool's budget), or code that must not
+ * take the device synchronisation cudaMalloc / cudaFree can cause.  Such a
+ * caller runs the row sweeps on its own buffers (fdp_apply_cells) and then
+ * reads the residues of its final state `d_main` (width x lanes, panel
+ * layout) into `d_residues` (lanes uint32 in device memory) with this call;
+ * `moduli` is host memory.  The dot product's 64-bit accumulators live in a
+ * fixed array inside the library (128 bytes, 16 lanes), so widths above 28
+ * or more than 16 lanes are rejected with FDP_ERR_ARGS.  The first call on a
+ * device, with that device current, looks the array up and copies a count
+ * table in; make that first call before any stream capture.  Every call on a
+ * device shares the array; each call clears it on `stream` first, but calls
+ * that overlap on the GPU race on it and must be serialised.
+ */
+fdp_status fdp_first_row_dot_noalloc(int width, int lanes, const uint32_t *moduli, const uint32_t *d_main,
+                                     uint32_t *d_residues, void *stream);
+
 /* Canonical rank / unrank of frontier words on the device (GB.cu:1568 rank_full). */
 fdp_status fdp_rank_words(fdp_ctx *ctx, int width, const uint64_t *d_words, uint64_t *d_ranks, uint64_t count,
                           void *stream);

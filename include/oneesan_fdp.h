@@ -76,6 +76,7 @@ typedef struct fdp_plan_out {
   uint64_t total_bytes;
   int rows;                         /* row sweeps per residue                     */
   int bounded_rows;                 /* of which in height-bounded spaces (prefix) */
+  int init_rows;                    /* rows of vertices filled by the row-k initialiser (default tuning) */
   int cells_per_row;                /* W - 1                                      */
   uint64_t alg_bytes_per_residue;   /* sum over cells of fdp_cell_bytes            */
   uint64_t transitions_per_residue; /* sum over cells of (M + D)                  */
@@ -175,8 +176,13 @@ fdp_status fdp_time_cells(fdp_ctx *ctx, const fdp_problem *problem, int rows, do
  * decode a chunk's items first and update them grouped by type (0 = the
  * default, 7; -1 = never); compact_items: states per lane of such a cell's
  * chunks, 1..4 (0 = automatic: 4 when the lanes fit one span of 8, else 2,
- * which leaves more of the SM's on-chip memory to L1).  Results never depend
- * on these settings.
+ * which leaves more of the SM's on-chip memory to L1); row_init_rows: the
+ * pass starts from the state after the first row_init_rows rows of vertices,
+ * computed directly by the row-k initialiser (a column automaton of that
+ * strip, the reference's row-5/row-6 initialisers, GB.cu:874-1032) instead of
+ * row sweeps, when its scratch fits the blocked state buffer (0 = automatic:
+ * 6 rows from width 14 up; -1 = never).  Results never depend on these
+ * settings.
  */
 typedef struct fdp_tuning {
   int block;
@@ -187,6 +193,7 @@ typedef struct fdp_tuning {
   int share_min;       /* shortest prefix decoded once per chunk (0: default)   */
   int compact_max_p;   /* highest cell grouped by centre type (0: default, -1: none) */
   int compact_items;   /* states per lane of a grouped chunk, 0..4 (0: automatic) */
+  int row_init_rows;   /* rows filled by the row-k initialiser, 2..7 (0: automatic, -1: none) */
 } fdp_tuning;
 fdp_status fdp_set_tuning(fdp_ctx *ctx, const fdp_tuning *tuning);
 fdp_status fdp_get_tuning(fdp_ctx *ctx, fdp_tuning *tuning);

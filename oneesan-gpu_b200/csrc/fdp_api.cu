@@ -9,6 +9,7 @@
 #include "fdp_api_internal.h"
 #include "fdp_host.h"
 #include "fdp_launch.h"
+#include "fdp_rowinit_dev.h"
 
 using fdp::DevTables;
 
@@ -79,18 +80,26 @@ extern "C" fdp_status fdp_plan(const fdp_problem *pr, uint64_t budget, fdp_plan_
   o.cells_per_row = W - 1;
   // Rows run in height-bounded spaces first (fdp_set_tuning bounded_prefix),
   // then in the full space.
+  // The first init_rows - 1 sweep rows are replaced by the row-k initialiser
+  // (default tuning: 6 rows of vertices from width 14 up, when its scratch fits).
   std::vector<int> caps;
   if (W >= 4) caps = fdp::bounded_prefix_caps(W);
-  o.bounded_rows = int(caps.size());
+  int R = W >= 14 ? (W - 1 < 6 ? W - 1 : 6) : 0;
+  if (R >= 2) {
+    const int cap = R <= int(caps.size()) ? caps[size_t(R - 1)] : FDP_FULL_CAP;
+    if (fdp::row_init_scratch(W, R, cap) > fdp::blocked_states(W)) R = 0;
+  }
+  o.init_rows = R;
+  const int first_row = R >= 2 ? R : 1;
+  o.bounded_rows = 0;
   o.alg_bytes_per_residue = 0;
   o.transitions_per_residue = 0;
-  for (int cap : caps) {
+  for (int row = first_row; row <= o.rows; ++row) {
+    const int cap = row <= int(caps.size()) ? caps[size_t(row - 1)] : FDP_FULL_CAP;
+    if (cap < FDP_FULL_CAP) ++o.bounded_rows;
     o.alg_bytes_per_residue += fdp::row_bytes(W, cap);
     o.transitions_per_residue += uint64_t(o.cells_per_row) * fdp::cell_transitions(W, cap);
   }
-  const int full_rows = o.rows - o.bounded_rows;
-  o.alg_bytes_per_residue += uint64_t(full_rows) * (W >= 2 ? fdp::row_bytes(W) : 0);
-  o.transitions_per_residue += uint64_t(full_rows) * uint64_t(o.cells_per_row) * fdp::cell_transitions(W);
   o.fits = o.total_bytes <= budget ? 1 : 0;
   *out = o;
   return FDP_OK;
@@ -160,11 +169,31 @@ fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const DevTables **out) {
   return fdp_ctx_tables_cap(c, W, FDP_FULL_CAP, out);
 }
 
+// Strip rows R the row-k initialiser fills directly for width W (0: the pass
+// starts from row 0), and the height cap of the space row R runs in.  Used
+// when the fill's scratch fits the blocked buffer (D words per lane, dead
+// before the first sweep).
+static int row_init_rows(const fdp_ctx *c, int W, int *cap) {
+  int R = c->cfg.row_init;
+  if (R == 0) R = W >= 14 ? 6 : 0;  // automatic
+  if (R < 2) return 0;
+  if (R > W - 1) R = W - 1;         // the state after row R-1 <= the last sweep row
+  if (R > 7) R = 7;
+  if (R < 2) return 0;
+  const std::vector<int> caps = (c->cfg.bounded_prefix && W >= 4) ? fdp::bounded_prefix_caps(W) : std::vector<int>{};
+  *cap = R <= int(caps.size()) ? caps[size_t(R - 1)] : FDP_FULL_CAP;
+  if (fdp::row_init_scratch(W, R, *cap) > fdp::blocked_states(W)) return 0;
+  return R;
+}
+
 // Every device table a residue pass of width W reads, uploaded before any
 // stream capture starts (allocation and blocking copies cannot be captured).
 fdp_status fdp_prepare_pass(fdp_ctx *c, int W, const DevTables **full) {
   fdp_status s = fdp_ctx_tables(c, W, full);
-  if (s != FDP_OK || !c->cfg.bounded_prefix || W < 4) return s;
+  if (s != FDP_OK) return s;
+  int rcap = 0;
+  if (const int R = row_init_rows(c, W, &rcap)) FDP_CK(fdp::prepare_row_init(W, R, rcap), "row-k initialiser tables");
+  if (!c->cfg.bounded_prefix || W < 4) return s;
   std::vector<int> caps = fdp::bounded_prefix_caps(W);
   caps.push_back(1);
   const DevTables *t = nullptr;
@@ -198,32 +227,50 @@ fdp_status fdp_enqueue_pass(fdp_ctx *c, const DevTables &t, int L, const uint32_
   const int W = t.W;
   const uint64_t M = fdp::main_states(W), D = fdp::blocked_states(W);
   uint64_t n = 0;
-  int first_full_row = 1;
-  if (c->cfg.bounded_prefix && W >= 4) {
-    const std::vector<int> caps = fdp::bounded_prefix_caps(W);
-    const DevTables *prev = nullptr;
-    fdp_status st = fdp_ctx_tables_cap(c, W, 1, &prev);
-    if (st != FDP_OK) return st;
+  fdp_status st = FDP_OK;
+  // Rows 1..B run in height-bounded spaces (caps[r-1] for row r), the rest in
+  // the full space.
+  const std::vector<int> caps = (c->cfg.bounded_prefix && W >= 4) ? fdp::bounded_prefix_caps(W) : std::vector<int>{};
+  const int B = int(caps.size());
+  auto space = [&](int cap, const DevTables **out) -> fdp_status {
+    if (cap >= FDP_FULL_CAP) {
+      *out = &t;
+      return FDP_OK;
+    }
+    return fdp_ctx_tables_cap(c, W, cap, out);
+  };
+  const DevTables *prev = nullptr;
+  int next_row = 1;
+  int rcap = 0;
+  if (const int R = row_init_rows(c, W, &rcap)) {
+    // Rows 0..R-1 at once: the state after row R-1, filled into row R's space
+    // (the blocked buffer is the fill's scratch).
+    if ((st = space(rcap, &prev)) != FDP_OK) return st;
+    FDP_CK(fdp::enqueue_row_init(W, R, rcap, L, mods, main, blk, D * uint64_t(L), s, &n), "row-k initialiser");
+    next_row = R;
+  } else if (B > 0) {
+    // Row 0 in the height-1 space: every word is a first-row state, coefficient 1.
+    if ((st = space(1, &prev)) != FDP_OK) return st;
     FDP_CK(fdp::launch_fill_ones(main, fdp::main_states_capped(W, 1) * uint64_t(L), s), "row-0 fill");
     ++n;
-    for (size_t r = 0; r < caps.size(); ++r) {
-      const DevTables *cur = nullptr;
-      if ((st = fdp_ctx_tables_cap(c, W, caps[r], &cur)) != FDP_OK) return st;
-      FDP_CK(fdp::enqueue_expand(*prev, *cur, L, main, blk, D * uint64_t(L), s, &n), "grow state");
-      for (int p = W - 1; p >= 1; --p) {
-        FDP_CK(fdp::launch_cell(*cur, L, mods, main, blk, p, p == W - 1, false, c->cfg, s), "bounded cell");
-        ++n;
-      }
-      prev = cur;
-    }
-    FDP_CK(fdp::enqueue_expand(*prev, t, L, main, blk, D * uint64_t(L), s, &n), "grow state");
-    first_full_row = int(caps.size()) + 1;
   } else {
     FDP_CK(cudaMemsetAsync(main, 0, size_t(M) * L * 4, s), "zero main");
     FDP_CK(fdp::launch_first_row_init(t, L, main, s), "row-0 init");
+    prev = &t;
     ++n;
   }
-  for (int row = first_full_row; row <= fdp::sweep_rows(W); ++row)
+  for (int row = next_row; row <= B && row <= fdp::sweep_rows(W); ++row) {
+    const DevTables *cur = nullptr;
+    if ((st = space(caps[size_t(row - 1)], &cur)) != FDP_OK) return st;
+    if (cur != prev) FDP_CK(fdp::enqueue_expand(*prev, *cur, L, main, blk, D * uint64_t(L), s, &n), "grow state");
+    for (int p = W - 1; p >= 1; --p) {
+      FDP_CK(fdp::launch_cell(*cur, L, mods, main, blk, p, p == W - 1, false, c->cfg, s), "bounded cell");
+      ++n;
+    }
+    prev = cur;
+  }
+  if (prev != &t) FDP_CK(fdp::enqueue_expand(*prev, t, L, main, blk, D * uint64_t(L), s, &n), "grow state");
+  for (int row = next_row > B + 1 ? next_row : B + 1; row <= fdp::sweep_rows(W); ++row)
     for (int p = W - 1; p >= 1; --p) {
       FDP_CK(fdp::launch_cell(t, L, mods, main, blk, p, p == W - 1, false, c->cfg, s), "cell");
       ++n;
@@ -394,10 +441,11 @@ void fdp_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   if (!c || !t) return FDP_ERR_ARGS;
   if (t->block < 64 || t->block > 256 || t->block % 32 || t->grid < 0 || t->lane_items < 0 || t->lane_items > 64 ||
-      t->share_min < 0 || t->compact_max_p < -1 || t->compact_items < 0 || t->compact_items > FDP_REC_MAX_ITEMS) {
+      t->share_min < 0 || t->compact_max_p < -1 || t->compact_items < 0 || t->compact_items > FDP_REC_MAX_ITEMS ||
+      t->row_init_rows < -1 || t->row_init_rows > 7) {
     g_last_error =
         "tuning: block must be a multiple of 32 in 64..256, grid >= 0, lane_items 0..64, share_min >= 0, "
-        "compact_max_p >= -1, compact_items 0..4";
+        "compact_max_p >= -1, compact_items 0..4, row_init_rows -1..7";
     return FDP_ERR_ARGS;
   }
   std::lock_guard<std::mutex> lk(c->mu);
@@ -409,6 +457,7 @@ extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   c->cfg.share_min = t->share_min > 0 ? t->share_min : fdp::LaunchCfg{}.share_min;
   c->cfg.compact_max_p = t->compact_max_p != 0 ? t->compact_max_p : fdp::LaunchCfg{}.compact_max_p;
   c->cfg.compact_items = t->compact_items;
+  c->cfg.row_init = t->row_init_rows;
   return FDP_OK;
 }
 
@@ -423,6 +472,7 @@ extern "C" fdp_status fdp_get_tuning(fdp_ctx *c, fdp_tuning *t) {
   t->share_min = c->cfg.share_min;
   t->compact_max_p = c->cfg.compact_max_p;
   t->compact_items = c->cfg.compact_items;
+  t->row_init_rows = c->cfg.row_init;
   return FDP_OK;
 }
 

@@ -1,0 +1,484 @@
+// Row-k initialiser, device half: the fill of fdp_rowinit.h on the GPU.
+//
+//   prefix levels : one warp per prefix, v_child[q'] = sum over the automaton
+//                   edges into q' of v_parent[q] x weight (mod p per lane);
+//   suffix levels : one warp per completion, u[q] = sum over the edges out of
+//                   q of weight x u_child[q'];
+//   products      : per end height h, out[base_x + j] = v_x . U_h[j] as a
+//                   tiled product of 64 prefixes x 64 completions.  The
+//                   suffix values are split into 16-bit halves so that every
+//                   partial sum of 32 x 16-bit products stays below 2^64 for
+//                   up to 2^16 terms; one Barrett reduction per output.
+// Scratch (two prefix levels, two suffix levels) is the caller's; the state
+// vector is written in the lane-panel layout of the cell kernels.
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "fdp_launch.h"
+#include "fdp_rowinit.h"
+#include "fdp_rowinit_dev.h"
+
+namespace fdp {
+
+namespace {
+
+constexpr int kH = 8;  // heights 0..7
+
+struct Lanes {
+  uint32_t p[16];
+  unsigned long long m[16];  // floor((2^64 - 1) / p)
+  uint64_t off[16];          // word offset of lane l's panel: L0 * N + (l - L0)
+  int pw[16];                // panel width of lane l
+};
+
+__device__ __forceinline__ uint32_t red64(unsigned long long x, uint32_t p, unsigned long long m) {
+  unsigned long long q = __umul64hi(x, m);
+  unsigned long long r = x - q * p;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    if (r >= p) r -= p;
+  return uint32_t(r);
+}
+
+struct AutDev {
+  const int *gid;         // [hoff[h] + q] -> global state id
+  const int *first_off;   // [3 + 1]
+  const int *first_to;    // local index
+  const uint32_t *first_w;
+  const int *fwd_off;     // [3 * (n + 1)] by (sym, target global id): edges into it
+  const int *fwd_from;    // local index of the source
+  const uint32_t *fwd_w;
+  const int *bwd_off;     // [3 * (n + 1)] by (sym, source global id): edges out of it
+  const int *bwd_to;      // local index of the target
+  const uint32_t *bwd_w;
+  const uint32_t *last_w; // [3 * n] by (sym, source global id)
+  int n;
+  int K[kH], hoff[kH];
+};
+
+struct LevelArgs {
+  uint64_t base[kH];  // word offset of height h's block (all lanes)
+  uint64_t cnt[kH];   // rows (prefix levels) or columns (suffix levels) of height h
+};
+
+__global__ void __launch_bounds__(256) rowinit_prefix_kernel(AutDev a, Lanes ln, int L, int first, int nprefix,
+                                                             const int32_t *parent, const uint8_t *sym,
+                                                             const uint8_t *height, const int32_t *row,
+                                                             const uint8_t *pheight, const int32_t *prow,
+                                                             LevelArgs cur, LevelArgs prev, const uint32_t *vin,
+                                                             uint32_t *vout) {
+  const int lane = threadIdx.x & 31;
+  const int warps = int((gridDim.x * blockDim.x) >> 5);
+  for (int i = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < nprefix; i += warps) {
+    const int h = height[i], s = sym[i], K = a.K[h];
+    const uint64_t ob = cur.base[h] + uint64_t(row[i]) * uint64_t(K);
+    const uint64_t lstride = cur.cnt[h] * uint64_t(K);
+    int hp = 0;
+    uint64_t ib = 0, istride = 0;
+    if (!first) {
+      const int pi = parent[i];
+      hp = pheight[pi];
+      ib = prev.base[hp] + uint64_t(prow[pi]) * uint64_t(a.K[hp]);
+      istride = prev.cnt[hp] * uint64_t(a.K[hp]);
+    }
+    for (int q = lane; q < K; q += 32) {
+      unsigned long long acc[16];
+      for (int l = 0; l < L; ++l) acc[l] = 0;
+      if (first) {
+        for (int e = a.first_off[s]; e < a.first_off[s + 1]; ++e)
+          if (a.first_to[e] == q)
+            for (int l = 0; l < L; ++l) acc[l] += a.first_w[e];
+      } else {
+        const int t = a.gid[a.hoff[h] + q];
+        const int *off = a.fwd_off + s * (a.n + 1);
+        for (int e = off[t]; e < off[t + 1]; ++e) {
+          const int src = a.fwd_from[e];
+          const uint32_t w = a.fwd_w[e];
+          for (int l = 0; l < L; ++l) acc[l] += (unsigned long long)vin[ib + uint64_t(l) * istride + src] * w;
+        }
+      }
+      for (int l = 0; l < L; ++l) vout[ob + uint64_t(l) * lstride + q] = red64(acc[l], ln.p[l], ln.m[l]);
+    }
+  }
+}
+
+// C[k][g] for the two suffix levels a kernel touches.
+struct SufCounts {
+  uint64_t cur[kH], prev[kH];
+};
+
+__global__ void __launch_bounds__(256) rowinit_suffix_kernel(AutDev a, Lanes ln, int L, int first_level, int hmax,
+                                                             SufCounts c, LevelArgs cur, LevelArgs prev,
+                                                             const uint32_t *uin, uint32_t *uout) {
+  const int lane = threadIdx.x & 31;
+  uint64_t total = 0;
+  for (int g = 0; g <= hmax; ++g) total += c.cur[g];
+  const uint64_t warps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t col = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; col < total; col += warps) {
+    int g = 0;
+    uint64_t j = col;
+    while (j >= c.cur[g]) j -= c.cur[g++];
+    const int K = a.K[g];
+    if (!K) continue;
+    const uint64_t ob = cur.base[g] + j * uint64_t(K);
+    const uint64_t lstride = cur.cnt[g] * uint64_t(K);
+    int s, gc = g;
+    uint64_t jc = j;
+    if (first_level) {
+      s = g == 0 ? 0 : 1;  // one position left: N from 0 or R from 1
+    } else if (jc < c.prev[g]) {
+      s = 0;
+    } else {
+      jc -= c.prev[g];
+      const uint64_t cr = g >= 1 ? c.prev[g - 1] : 0;
+      if (jc < cr) {
+        s = 1;
+        gc = g - 1;
+      } else {
+        jc -= cr;
+        s = 2;
+        gc = g + 1;
+      }
+    }
+    for (int q = lane; q < K; q += 32) {
+      const int src = a.gid[a.hoff[g] + q];
+      unsigned long long acc[16];
+      for (int l = 0; l < L; ++l) acc[l] = 0;
+      if (first_level) {
+        const uint32_t w = a.last_w[s * a.n + src];
+        for (int l = 0; l < L; ++l) acc[l] = w;
+      } else if (gc <= hmax) {
+        const uint64_t ib = prev.base[gc] + jc * uint64_t(a.K[gc]);
+        const uint64_t istride = prev.cnt[gc] * uint64_t(a.K[gc]);
+        const int *off = a.bwd_off + s * (a.n + 1);
+        for (int e = off[src]; e < off[src + 1]; ++e) {
+          const int dst = a.bwd_to[e];
+          const uint32_t w = a.bwd_w[e];
+          for (int l = 0; l < L; ++l) acc[l] += (unsigned long long)uin[ib + uint64_t(l) * istride + dst] * w;
+        }
+      }
+      for (int l = 0; l < L; ++l) uout[ob + uint64_t(l) * lstride + q] = red64(acc[l], ln.p[l], ln.m[l]);
+    }
+  }
+}
+
+// out[base[i] + j] = V[i] . U[j] for one end height: V is n rows x K, U is C
+// columns x K (both K-contiguous, per lane at stride n*K / C*K).
+constexpr int TM = 64, TN = 64, TQ = 16;
+__global__ void __launch_bounds__(256) rowinit_product_kernel(Lanes ln, int L, int K, uint64_t n, uint64_t C,
+                                                              const uint32_t *V, const uint32_t *U,
+                                                              const uint64_t *base, uint32_t *out) {
+  __shared__ __align__(16) uint32_t As[TQ][TM], Bl[TQ][TN], Bh[TQ][TN];
+  const uint64_t tiles_n = (C + TN - 1) / TN;
+  const uint64_t tile = blockIdx.x;
+  const uint64_t i0 = (tile / tiles_n) * TM, j0 = (tile % tiles_n) * TN;
+  const int t = threadIdx.x, ty = t >> 4, tx = t & 15;
+  for (int l = 0; l < L; ++l) {
+    const uint32_t *Vl = V + uint64_t(l) * n * uint64_t(K);
+    const uint32_t *Ul = U + uint64_t(l) * C * uint64_t(K);
+    unsigned long long lo[4][4], hi[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) lo[r][c] = hi[r][c] = 0;
+    for (int q0 = 0; q0 < K; q0 += TQ) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int e = t + 256 * r, rr = e / TQ, qq = e % TQ;
+        const uint64_t gi = i0 + uint64_t(rr), gj = j0 + uint64_t(rr);
+        const int gq = q0 + qq;
+        As[qq][rr] = (gi < n && gq < K) ? Vl[gi * uint64_t(K) + uint64_t(gq)] : 0u;
+        const uint32_t b = (gj < C && gq < K) ? Ul[gj * uint64_t(K) + uint64_t(gq)] : 0u;
+        Bl[qq][rr] = b & 0xffffu;
+        Bh[qq][rr] = b >> 16;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int qq = 0; qq < TQ; ++qq) {
+        const uint4 av = *reinterpret_cast<const uint4 *>(&As[qq][ty * 4]);
+        const uint4 bl = *reinterpret_cast<const uint4 *>(&Bl[qq][tx * 4]);
+        const uint4 bh = *reinterpret_cast<const uint4 *>(&Bh[qq][tx * 4]);
+        const uint32_t ar[4] = {av.x, av.y, av.z, av.w}, blr[4] = {bl.x, bl.y, bl.z, bl.w},
+                       bhr[4] = {bh.x, bh.y, bh.z, bh.w};
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            lo[r][c] += (unsigned long long)ar[r] * blr[c];
+            hi[r][c] += (unsigned long long)ar[r] * bhr[c];
+          }
+      }
+      __syncthreads();
+    }
+    const uint32_t p = ln.p[l];
+    const unsigned long long m = ln.m[l];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint64_t gi = i0 + uint64_t(ty * 4 + r);
+      if (gi >= n) continue;
+      const uint64_t b0 = base[gi];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const uint64_t gj = j0 + uint64_t(tx * 4 + c);
+        if (gj >= C) continue;
+        const unsigned long long h16 = (unsigned long long)red64(hi[r][c], p, m) << 16;
+        const uint32_t v = red64(red64(lo[r][c], p, m) + h16, p, m);
+        out[ln.off[l] + (b0 + gj) * uint64_t(ln.pw[l])] = v;
+      }
+    }
+  }
+}
+
+struct RowInitDevice {
+  RowInitPlan plan;
+  AutDev aut{};
+  std::vector<void *> allocs;
+  // prefix levels (concatenated) and per-level offsets
+  std::vector<size_t> lvl_off;  // prefixes before level k (size P + 1)
+  int32_t *parent = nullptr, *row = nullptr;
+  uint8_t *sym = nullptr, *height = nullptr;
+  uint64_t *base_hr = nullptr;  // level P bases by (height, row)
+  std::vector<uint64_t> base_hoff;
+  ~RowInitDevice() {
+    for (void *p : allocs) cudaFree(p);
+  }
+};
+
+template <typename T>
+cudaError_t upload(RowInitDevice &d, const std::vector<T> &h, T **out) {
+  *out = nullptr;
+  const size_t bytes = std::max<size_t>(1, h.size()) * sizeof(T);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(out), bytes);
+  if (e != cudaSuccess) return e;
+  d.allocs.push_back(*out);
+  if (h.empty()) return cudaSuccess;
+  return cudaMemcpy(*out, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+cudaError_t build_device(int W, int rows, int cap, std::unique_ptr<RowInitDevice> &out) {
+  auto d = std::make_unique<RowInitDevice>();
+  d->plan = plan_row_init(W, rows, cap);
+  const RowInitPlan &pl = d->plan;
+  const RowAutomaton &a = row_automaton(rows);
+  AutDev &ad = d->aut;
+  ad.n = a.nstates;
+  int acc = 0;
+  for (int h = 0; h < kH; ++h) {
+    ad.K[h] = h <= rows ? a.per_height[size_t(h)] : 0;
+    ad.hoff[h] = acc;
+    acc += ad.K[h];
+  }
+  std::vector<int> gid(size_t(std::max(acc, 1)), 0);
+  for (int s = 0; s < a.nstates; ++s) gid[size_t(ad.hoff[a.height[size_t(s)]] + a.index[size_t(s)])] = s;
+  std::vector<int> first_off(4, 0), first_to;
+  std::vector<uint32_t> first_w;
+  for (int s = 0; s < 3; ++s) {
+    for (const AutTrans &t : a.first[s]) {
+      first_to.push_back(a.index[size_t(t.to)]);
+      first_w.push_back(t.weight);
+    }
+    first_off[size_t(s) + 1] = int(first_to.size());
+  }
+  std::vector<int> fwd_off(size_t(3) * (a.nstates + 1), 0), fwd_from, bwd_off(size_t(3) * (a.nstates + 1), 0), bwd_to;
+  std::vector<uint32_t> fwd_w, bwd_w, last_w(size_t(3) * a.nstates, 0);
+  for (int s = 0; s < 3; ++s) {
+    std::vector<std::vector<std::pair<int, uint32_t>>> in(size_t(a.nstates)), outv(size_t(a.nstates));
+    for (const AutTrans &t : a.inner[s]) {
+      in[size_t(t.to)].push_back({a.index[size_t(t.from)], t.weight});
+      outv[size_t(t.from)].push_back({a.index[size_t(t.to)], t.weight});
+    }
+    int *fo = fwd_off.data() + size_t(s) * (a.nstates + 1), *bo = bwd_off.data() + size_t(s) * (a.nstates + 1);
+    fo[0] = int(fwd_from.size());
+    bo[0] = int(bwd_to.size());
+    for (int q = 0; q < a.nstates; ++q) {
+      for (auto &e : in[size_t(q)]) {
+        fwd_from.push_back(e.first);
+        fwd_w.push_back(e.second);
+      }
+      fo[q + 1] = int(fwd_from.size());
+      for (auto &e : outv[size_t(q)]) {
+        bwd_to.push_back(e.first);
+        bwd_w.push_back(e.second);
+      }
+      bo[q + 1] = int(bwd_to.size());
+    }
+    for (const AutTrans &t : a.last[s]) last_w[size_t(s) * a.nstates + size_t(t.from)] += t.weight;
+  }
+  cudaError_t e;
+#define UP(vec, ptr)                                                      \
+  if ((e = upload(*d, vec, &ptr)) != cudaSuccess) return e;
+  int *p_gid, *p_fo, *p_ft, *p_fwo, *p_fwf, *p_bwo, *p_bwt;
+  uint32_t *p_fw, *p_fww, *p_bww, *p_lw;
+  UP(gid, p_gid) UP(first_off, p_fo) UP(first_to, p_ft) UP(first_w, p_fw) UP(fwd_off, p_fwo) UP(fwd_from, p_fwf)
+  UP(fwd_w, p_fww) UP(bwd_off, p_bwo) UP(bwd_to, p_bwt) UP(bwd_w, p_bww) UP(last_w, p_lw)
+  ad.gid = p_gid;
+  ad.first_off = p_fo;
+  ad.first_to = p_ft;
+  ad.first_w = p_fw;
+  ad.fwd_off = p_fwo;
+  ad.fwd_from = p_fwf;
+  ad.fwd_w = p_fww;
+  ad.bwd_off = p_bwo;
+  ad.bwd_to = p_bwt;
+  ad.bwd_w = p_bww;
+  ad.last_w = p_lw;
+  // Prefix levels.
+  std::vector<int32_t> par, rw;
+  std::vector<uint8_t> sy, hh;
+  d->lvl_off.assign(1, 0);
+  for (int k = 0; k < pl.P; ++k) {
+    par.insert(par.end(), pl.parent[size_t(k)].begin(), pl.parent[size_t(k)].end());
+    rw.insert(rw.end(), pl.row[size_t(k)].begin(), pl.row[size_t(k)].end());
+    sy.insert(sy.end(), pl.sym[size_t(k)].begin(), pl.sym[size_t(k)].end());
+    hh.insert(hh.end(), pl.height[size_t(k)].begin(), pl.height[size_t(k)].end());
+    d->lvl_off.push_back(par.size());
+  }
+  UP(par, d->parent) UP(rw, d->row) UP(sy, d->sym) UP(hh, d->height)
+  // Level-P bases by (height, row).
+  const auto &htop = pl.height[size_t(pl.P - 1)];
+  const auto &rtop = pl.row[size_t(pl.P - 1)];
+  d->base_hoff.assign(kH + 1, 0);
+  for (int h = 0; h < kH; ++h)
+    d->base_hoff[size_t(h) + 1] = d->base_hoff[size_t(h)] + (h <= rows ? pl.rows_of[size_t(pl.P - 1)][size_t(h)] : 0);
+  std::vector<uint64_t> bhr(size_t(d->base_hoff[kH]), 0);
+  for (size_t i = 0; i < htop.size(); ++i) bhr[size_t(d->base_hoff[htop[i]]) + size_t(rtop[i])] = pl.base[i];
+  UP(bhr, d->base_hr)
+#undef UP
+  out = std::move(d);
+  return cudaSuccess;
+}
+
+std::mutex g_mu;
+std::map<std::tuple<int, int, int, int>, std::unique_ptr<RowInitDevice>> g_cache;  // (device, W, rows, cap)
+
+LevelArgs level_args(const std::vector<uint64_t> &cnt, const int *K, int hmax, int L) {
+  LevelArgs a{};
+  uint64_t off = 0;
+  for (int h = 0; h < kH; ++h) {
+    a.cnt[h] = h <= hmax && h < int(cnt.size()) ? cnt[size_t(h)] : 0;
+    a.base[h] = off;
+    off += a.cnt[h] * uint64_t(K[h]) * uint64_t(L);
+  }
+  return a;
+}
+
+}  // namespace
+
+cudaError_t prepare_row_init(int W, int rows, int cap) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto key = std::make_tuple(dev, W, rows, cap);
+  if (g_cache.count(key)) return cudaSuccess;
+  std::unique_ptr<RowInitDevice> d;
+  if ((e = build_device(W, rows, cap, d)) != cudaSuccess) return e;
+  g_cache.emplace(key, std::move(d));
+  return cudaSuccess;
+}
+
+uint64_t row_init_scratch(int W, int rows, int cap) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int>, uint64_t> words;
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_tuple(W, rows, cap);
+  auto it = words.find(key);
+  if (it == words.end()) it = words.emplace(key, row_init_scratch_words(plan_row_init(W, rows, cap))).first;
+  return it->second;
+}
+
+cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mods, uint32_t *main,
+                             uint32_t *scratch, uint64_t scratch_words, cudaStream_t s, uint64_t *launches) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  RowInitDevice *d = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_cache.find(std::make_tuple(dev, W, rows, cap));
+    if (it == g_cache.end()) return cudaErrorNotReady;  // prepare_row_init first (outside capture)
+    d = it->second.get();
+  }
+  const RowInitPlan &pl = d->plan;
+  if (L < 1 || L > 16) return cudaErrorInvalidValue;
+  if (row_init_scratch_words(pl) * uint64_t(L) > scratch_words) return cudaErrorInvalidValue;
+  Lanes ln{};
+  for (int l = 0; l < L;) {
+    const int pw = (L - l >= 8) ? 8 : (L - l >= 4) ? 4 : (L - l >= 2) ? 2 : 1;
+    for (int i = 0; i < pw; ++i) {
+      ln.off[l + i] = uint64_t(l) * pl.states + uint64_t(i);
+      ln.pw[l + i] = pw;
+    }
+    l += pw;
+  }
+  for (int l = 0; l < L; ++l) {
+    ln.p[l] = mods[l];
+    ln.m[l] = ~0ull / mods[l];
+  }
+  uint64_t pre_words = 0, suf_words = 0;
+  for (int k = 0; k < pl.P; ++k) {
+    uint64_t w = 0;
+    for (int h = 0; h <= pl.hmax; ++h) w += pl.rows_of[size_t(k)][size_t(h)] * uint64_t(pl.K[size_t(h)]);
+    pre_words = std::max(pre_words, w * uint64_t(L));
+  }
+  for (int k = 1; k <= pl.S; ++k) {
+    uint64_t w = 0;
+    for (int g = 0; g <= pl.hmax; ++g) w += pl.C[size_t(k)][size_t(g)] * uint64_t(pl.K[size_t(g)]);
+    suf_words = std::max(suf_words, w * uint64_t(L));
+  }
+  uint32_t *pre[2] = {scratch, scratch + pre_words};
+  uint32_t *suf[2] = {scratch + 2 * pre_words, scratch + 2 * pre_words + suf_words};
+  if ((e = cudaMemsetAsync(main, 0, size_t(pl.states) * L * 4, s)) != cudaSuccess) return e;
+  const int blocks = device_sm_count() * 8;
+  uint64_t n = 0;
+  // Prefix levels 1..P.
+  LevelArgs prevA{};
+  for (int k = 1; k <= pl.P; ++k) {
+    const LevelArgs cur = level_args(pl.rows_of[size_t(k - 1)], d->aut.K, pl.hmax, L);
+    const size_t o = d->lvl_off[size_t(k - 1)], po = k > 1 ? d->lvl_off[size_t(k - 2)] : 0;
+    const int np = int(d->lvl_off[size_t(k)] - o);
+    rowinit_prefix_kernel<<<blocks, 256, 0, s>>>(d->aut, ln, L, k == 1, np, d->parent + o, d->sym + o, d->height + o,
+                                                 d->row + o, d->height + po, d->row + po, cur, prevA,
+                                                 pre[(k + 1) & 1], pre[k & 1]);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    ++n;
+    prevA = cur;
+  }
+  // Suffix levels 1..S.
+  LevelArgs prevU{};
+  for (int k = 1; k <= pl.S; ++k) {
+    std::vector<uint64_t> cnt(pl.C[size_t(k)].begin(), pl.C[size_t(k)].end());
+    const LevelArgs cur = level_args(cnt, d->aut.K, pl.hmax, L);
+    SufCounts sc{};
+    for (int g = 0; g < kH; ++g) {
+      sc.cur[g] = g <= pl.hmax ? pl.C[size_t(k)][size_t(g)] : 0;
+      sc.prev[g] = (k > 1 && g <= pl.hmax) ? pl.C[size_t(k - 1)][size_t(g)] : 0;
+    }
+    rowinit_suffix_kernel<<<blocks, 256, 0, s>>>(d->aut, ln, L, k == 1, pl.hmax, sc, cur, prevU, suf[(k + 1) & 1],
+                                                 suf[k & 1]);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    ++n;
+    prevU = cur;
+  }
+  // Products, one launch per end height.
+  const uint32_t *V = pre[pl.P & 1], *U = suf[pl.S & 1];
+  for (int h = 0; h <= pl.hmax; ++h) {
+    const uint64_t rows_h = prevA.cnt[h], cols = prevU.cnt[h];
+    const int K = d->aut.K[h];
+    if (!rows_h || !cols || !K) continue;
+    const uint64_t tiles = ((rows_h + TM - 1) / TM) * ((cols + TN - 1) / TN);
+    rowinit_product_kernel<<<unsigned(tiles), 256, 0, s>>>(ln, L, K, rows_h, cols, V + prevA.base[h],
+                                                           U + prevU.base[h], d->base_hr + d->base_hoff[size_t(h)],
+                                                           main);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    ++n;
+  }
+  if (launches) *launches += n;
+  return cudaSuccess;
+}
+
+}  // namespace fdp

@@ -74,13 +74,13 @@ int main(int argc, char **argv) {
   }
   if (const char *e = getenv("GRIDFP_PLAN_ONLY"); e && atoi(e) != 0) {
     fprintf(stderr,
-            "PLAN n=%d W=%d gpus=1 main=%llu blocked=%llu auth_gib=%.6f lanes=%d passes=%d index_bits=%d "
+            "PLAN n=%d W=%d gpus=1 main=%llu blocked=%llu auth_gib=%.6f lanes=%d passes=%d index_bits=%d init_rows=%d "
             "state_gib=%.6f scratch_gib=0 table_mib=%.3f total_gib=%.6f rows=%d cells_per_row=%d "
             "alg_bytes_per_residue=%llu transitions_per_residue=%llu scratch_limit_mib=%d max_window=%d "
             "scratch_fits=1\n",
             n, plan.width, (unsigned long long)plan.main_states, (unsigned long long)plan.blocked_states,
             double(plan.main_states + plan.blocked_states) * 4.0 / double(1ull << 30), plan.lanes, plan.passes,
-            plan.index_bits, double(plan.state_bytes) / double(1ull << 30), double(plan.table_bytes) / (1 << 20),
+            plan.index_bits, plan.init_rows, double(plan.state_bytes) / double(1ull << 30), double(plan.table_bytes) / (1 << 20),
             double(plan.total_bytes) / double(1ull << 30), plan.rows, plan.cells_per_row,
             (unsigned long long)plan.alg_bytes_per_residue, (unsigned long long)plan.transitions_per_residue,
             target_mib, max_window);

@@ -85,10 +85,26 @@ def test_autotune_picks_a_correct_configuration(engine):
 def test_bounded_prefix_equals_full_rows(engine):
     try:
         for n, mods in ((4, P[:1]), (9, P[:2]), (15, P[:5]), (16, P[:14])):
-            engine.set_tuning(bounded_prefix=False)
+            engine.set_tuning(bounded_prefix=False, row_init_rows=-1)
             full = engine.residues(n, mods, lanes=len(mods)).residues
-            engine.set_tuning(bounded_prefix=True)
+            engine.set_tuning(bounded_prefix=True, row_init_rows=-1)
             assert engine.residues(n, mods, lanes=len(mods)).residues == full, n
             assert engine.residues(n, mods, lanes=1).residues == full, n
+    finally:
+        engine.set_tuning()
+
+
+@pytest.mark.parametrize("rows", [2, 3, 4, 5, 6, 7])
+def test_row_init_equals_row_sweeps(engine, rows):
+    """The row-k initialiser (the state after the first `rows` rows of
+    vertices, computed by the column automaton) gives the residues of the row
+    sweeps, in the bounded and the full space, for every lane count kind."""
+    try:
+        for n, mods, lanes in ((6, P[:2], 2), (9, [2, 3, P[0]], 3), (12, P[:8], 8), (14, P[:14], 14), (15, P[:3], 1)):
+            engine.set_tuning(row_init_rows=-1)
+            want = engine.residues(n, mods, lanes=lanes).residues
+            for bounded in (True, False):
+                engine.set_tuning(bounded_prefix=bounded, row_init_rows=rows)
+                assert engine.residues(n, mods, lanes=lanes).residues == want, (n, rows, bounded)
     finally:
         engine.set_tuning()

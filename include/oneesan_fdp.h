@@ -181,8 +181,9 @@ fdp_status fdp_time_cells(fdp_ctx *ctx, const fdp_problem *problem, int rows, do
  * computed directly by the row-k initialiser (a column automaton of that
  * strip, the reference's row-5/row-6 initialisers, GB.cu:874-1032) instead of
  * row sweeps, when its scratch fits the blocked state buffer (0 = automatic:
- * 6 rows from width 14 up; -1 = never).  Results never depend on these
- * settings.
+ * 7 rows from width 18 up, 6 from width 14; -1 = never); row_init_product:
+ * the initialiser's products on the tensor cores (0, tcgen05 with 8-bit limbs)
+ * or on the CUDA cores (1).  Results never depend on these settings.
  */
 typedef struct fdp_tuning {
   int block;
@@ -194,6 +195,7 @@ typedef struct fdp_tuning {
   int compact_max_p;   /* highest cell grouped by centre type (0: default, -1: none) */
   int compact_items;   /* states per lane of a grouped chunk, 0..4 (0: automatic) */
   int row_init_rows;   /* rows filled by the row-k initialiser, 2..7 (0: automatic, -1: none) */
+  int row_init_product; /* its products on the tensor cores (0, default) or CUDA cores (1) */
 } fdp_tuning;
 fdp_status fdp_set_tuning(fdp_ctx *ctx, const fdp_tuning *tuning);
 fdp_status fdp_get_tuning(fdp_ctx *ctx, fdp_tuning *tuning);

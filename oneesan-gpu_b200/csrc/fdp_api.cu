@@ -81,10 +81,11 @@ extern "C" fdp_status fdp_plan(const fdp_problem *pr, uint64_t budget, fdp_plan_
   // Rows run in height-bounded spaces first (fdp_set_tuning bounded_prefix),
   // then in the full space.
   // The first init_rows - 1 sweep rows are replaced by the row-k initialiser
-  // (default tuning: 6 rows of vertices from width 14 up, when its scratch fits).
+  // (default tuning, when its scratch fits).
   std::vector<int> caps;
   if (W >= 4) caps = fdp::bounded_prefix_caps(W);
-  int R = W >= 14 ? (W - 1 < 6 ? W - 1 : 6) : 0;
+  int R = fdp::auto_row_init_rows(W);
+  if (R > W - 1) R = W - 1;
   if (R >= 2) {
     const int cap = R <= int(caps.size()) ? caps[size_t(R - 1)] : FDP_FULL_CAP;
     if (fdp::row_init_scratch(W, R, cap) > fdp::blocked_states(W)) R = 0;
@@ -175,7 +176,7 @@ fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const DevTables **out) {
 // before the first sweep).
 static int row_init_rows(const fdp_ctx *c, int W, int *cap) {
   int R = c->cfg.row_init;
-  if (R == 0) R = W >= 14 ? 6 : 0;  // automatic
+  if (R == 0) R = fdp::auto_row_init_rows(W);
   if (R < 2) return 0;
   if (R > W - 1) R = W - 1;         // the state after row R-1 <= the last sweep row
   if (R > 7) R = 7;
@@ -246,7 +247,8 @@ fdp_status fdp_enqueue_pass(fdp_ctx *c, const DevTables &t, int L, const uint32_
     // Rows 0..R-1 at once: the state after row R-1, filled into row R's space
     // (the blocked buffer is the fill's scratch).
     if ((st = space(rcap, &prev)) != FDP_OK) return st;
-    FDP_CK(fdp::enqueue_row_init(W, R, rcap, L, mods, main, blk, D * uint64_t(L), s, &n), "row-k initialiser");
+    FDP_CK(fdp::enqueue_row_init(W, R, rcap, L, mods, main, blk, D * uint64_t(L), c->cfg.row_init_tensor, s, &n),
+           "row-k initialiser");
     next_row = R;
   } else if (B > 0) {
     // Row 0 in the height-1 space: every word is a first-row state, coefficient 1.
@@ -330,6 +332,14 @@ extern "C" fdp_status fdp_run_sync(fdp_ctx *c, const fdp_problem *pr, uint32_t *
   cudaGraphExecDestroy(ge);
   FDP_CK(ce, "graph launch");
   FDP_CK(se, "residue pass");
+  {
+    int rcap = 0;
+    const int R = row_init_rows(c, W, &rcap);
+    if (R && c->cfg.row_init_tensor && fdp::row_init_failed(W, R, rcap)) {
+      g_last_error = "row-k initialiser: a bounded wait of the tensor-core product gave up";
+      return FDP_ERR_CUDA;
+    }
+  }
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   acc.device_s = ms * 1e-3;
@@ -442,10 +452,10 @@ extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   if (!c || !t) return FDP_ERR_ARGS;
   if (t->block < 64 || t->block > 256 || t->block % 32 || t->grid < 0 || t->lane_items < 0 || t->lane_items > 64 ||
       t->share_min < 0 || t->compact_max_p < -1 || t->compact_items < 0 || t->compact_items > FDP_REC_MAX_ITEMS ||
-      t->row_init_rows < -1 || t->row_init_rows > 7) {
+      t->row_init_rows < -1 || t->row_init_rows > 7 || t->row_init_product < 0 || t->row_init_product > 1) {
     g_last_error =
         "tuning: block must be a multiple of 32 in 64..256, grid >= 0, lane_items 0..64, share_min >= 0, "
-        "compact_max_p >= -1, compact_items 0..4, row_init_rows -1..7";
+        "compact_max_p >= -1, compact_items 0..4, row_init_rows -1..7, row_init_product 0..1";
     return FDP_ERR_ARGS;
   }
   std::lock_guard<std::mutex> lk(c->mu);
@@ -458,6 +468,7 @@ extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   c->cfg.compact_max_p = t->compact_max_p != 0 ? t->compact_max_p : fdp::LaunchCfg{}.compact_max_p;
   c->cfg.compact_items = t->compact_items;
   c->cfg.row_init = t->row_init_rows;
+  c->cfg.row_init_tensor = t->row_init_product == 0;
   return FDP_OK;
 }
 
@@ -473,6 +484,7 @@ extern "C" fdp_status fdp_get_tuning(fdp_ctx *c, fdp_tuning *t) {
   t->compact_max_p = c->cfg.compact_max_p;
   t->compact_items = c->cfg.compact_items;
   t->row_init_rows = c->cfg.row_init;
+  t->row_init_product = c->cfg.row_init_tensor ? 0 : 1;
   return FDP_OK;
 }
 

@@ -33,6 +33,7 @@ struct LaunchCfg {
   int compact_items = 0;     // states per lane of a compacted chunk (1..FDP_REC_MAX_ITEMS; 0: 4 for
                              // one span, 2 when closure sources are staged, which leaves L1 room)
   int row_init = 0;          // strip rows filled directly by the row-k initialiser (0: automatic, -1: never)
+  bool row_init_tensor = true;  // the initialiser's products on the tensor cores (else the CUDA cores)
 };
 
 template <typename Idx, int K>

@@ -233,6 +233,177 @@ __global__ void __launch_bounds__(256) rowinit_product_kernel(Lanes ln, int L, i
   }
 }
 
+// The same products on the 5th-generation tensor cores (tcgen05, kind::i8).
+// Every value is split into four u8 limbs, v = sum_i 2^(8i) v_i; the 16 limb
+// products accumulate by shift s = i + j into seven s32 accumulators in tensor
+// memory (7 x 64 of the 512 columns), so out = sum_s 2^(8s) G_s mod p.  A
+// group sums at most 4 x K x 255^2 < 2^31 for K <= 8192.  Tiles of 128
+// prefixes x 64 completions, K in steps of 32 bytes; each thread splits its
+// row's values into the limbs' shared-memory tiles (K-major, no swizzle:
+// core matrices of 8 rows x 16 bytes, 256 bytes between 8-row groups, 128
+// bytes between the two 16-byte K halves), one thread issues the MMAs and
+// commits them to an mbarrier that every thread waits on (bounded).  One CTA
+// per SM (it holds all 512 tensor-memory columns), persistent over
+// (tile, lane) items; all lanes of a tile run back to back.
+constexpr int MM = 128, MN = 64, MK = 32;
+constexpr int A_LIMB = MM * MK, B_LIMB = MN * MK;  // bytes of one limb's tile per K step
+constexpr uint32_t kIdescI8 = (2u << 4) | (uint32_t(MN >> 3) << 17) | (uint32_t(MM >> 4) << 24);  // S32 += U8 x U8, K-major
+constexpr uint32_t kTmemCols = 512;
+constexpr size_t kMmaSmem = 120 * 1024;  // more than half an SM's shared memory: one CTA per SM
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  return uint64_t((saddr >> 4) & 0x3fffu) | (uint64_t(128 >> 4) << 16) | (uint64_t(256 >> 4) << 32) |
+         (uint64_t(1) << 46);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Row `row` of a 128- or 64-row operand tile: 32 values -> 4 limb tiles.
+__device__ __forceinline__ void stage_row(unsigned char *tile, int limb_bytes, int row, const uint32_t *src, int k0,
+                                          int K, bool valid) {
+  uint32_t v[MK];
+#pragma unroll
+  for (int k = 0; k < MK; ++k) v[k] = (valid && k0 + k < K) ? src[k0 + k] : 0u;
+  const int roff = (row >> 3) * 256 + (row & 7) * 16;
+#pragma unroll
+  for (int limb = 0; limb < 4; ++limb) {
+    const int sh = 8 * limb;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      uint32_t w[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int k = c * 16 + q * 4;
+        w[q] = ((v[k] >> sh) & 0xffu) | (((v[k + 1] >> sh) & 0xffu) << 8) | (((v[k + 2] >> sh) & 0xffu) << 16) |
+               (((v[k + 3] >> sh) & 0xffu) << 24);
+      }
+      *reinterpret_cast<uint4 *>(tile + limb * limb_bytes + roff + c * 128) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128, 1) rowinit_mma_kernel(Lanes ln, int L, int K, uint64_t n, uint64_t C,
+                                                             const uint32_t *V, const uint32_t *U,
+                                                             const uint64_t *base, uint32_t *out,
+                                                             unsigned int *err) {
+  extern __shared__ __align__(1024) unsigned char dsm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  unsigned char *sA = dsm, *sB = dsm + 4 * A_LIMB;
+  const int t = threadIdx.x, warp = t >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1) : "memory");
+    abort_flag = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot, bar = smem_addr(&mbar);
+  uint32_t phase = 0;
+  const uint64_t tiles_n = (C + MN - 1) / MN, tiles = ((n + MM - 1) / MM) * tiles_n;
+  const uint64_t items = tiles * uint64_t(L);
+  const int nks = (K + MK - 1) / MK;
+  for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const uint64_t tile = it / uint64_t(L);
+    const int l = int(it % uint64_t(L));
+    const uint64_t i0 = (tile / tiles_n) * MM, j0 = (tile % tiles_n) * MN;
+    const uint32_t *Vl = V + uint64_t(l) * n * uint64_t(K), *Ul = U + uint64_t(l) * C * uint64_t(K);
+    const uint64_t gi = i0 + uint64_t(t);
+    for (int ks = 0; ks < nks; ++ks) {
+      stage_row(sA, A_LIMB, t, Vl + (gi < n ? gi : 0) * uint64_t(K), ks * MK, K, gi < n);
+      if (t < MN) {
+        const uint64_t gj = j0 + uint64_t(t);
+        stage_row(sB, B_LIMB, t, Ul + (gj < C ? gj : 0) * uint64_t(K), ks * MK, K, gj < C);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (t == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int sft = i + j;
+            const uint32_t en = (ks > 0 || i != (sft > 3 ? sft - 3 : 0)) ? 1u : 0u;
+            const uint64_t da = umma_desc(smem_addr(sA + i * A_LIMB)), db = umma_desc(smem_addr(sB + j * B_LIMB));
+            asm volatile(
+                "{\n\t.reg .pred PRED_enable_input_d;\n\t"
+                "setp.ne.b32 PRED_enable_input_d, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, PRED_enable_input_d;\n\t}"
+                :
+                : "r"(tmem + uint32_t(sft * MN)), "l"(da), "l"(db), "r"(kIdescI8), "r"(en)
+                : "memory");
+          }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                     : "memory");
+      }
+      // The MMAs read the staged tiles: wait for them before the next stage.
+      if (!mbar_wait(bar, phase)) atomicExch(&abort_flag, 1);
+      phase ^= 1u;
+      __syncthreads();
+      if (abort_flag) break;
+    }
+    if (abort_flag) break;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // Rows 32w..32w+31 of the tile are tensor-memory lanes of warp w.
+    const uint32_t p = ln.p[l];
+    const unsigned long long m = ln.m[l];
+    const uint64_t b0 = gi < n ? base[gi] : 0;
+    for (int c = 0; c < MN; c += 16) {
+      unsigned long long acc[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc[q] = 0;
+      for (int sft = 6; sft >= 0; --sft) {
+        uint32_t g[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];"
+            : "=r"(g[0]), "=r"(g[1]), "=r"(g[2]), "=r"(g[3]), "=r"(g[4]), "=r"(g[5]), "=r"(g[6]), "=r"(g[7]),
+              "=r"(g[8]), "=r"(g[9]), "=r"(g[10]), "=r"(g[11]), "=r"(g[12]), "=r"(g[13]), "=r"(g[14]), "=r"(g[15])
+            : "r"(tmem + (uint32_t(warp * 32) << 16) + uint32_t(sft * MN + c)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[q] = red64(acc[q] * 256ull + g[q], p, m);
+      }
+      if (gi < n) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const uint64_t gj = j0 + uint64_t(c + q);
+          if (gj < C) out[ln.off[l] + (b0 + gj) * uint64_t(ln.pw[l])] = uint32_t(acc[q]);
+        }
+      }
+    }
+    // Every read of the accumulators is done before the next item's MMAs.
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  if (t == 0 && abort_flag) atomicExch(err, 1u);
+}
+
 struct RowInitDevice {
   RowInitPlan plan;
   AutDev aut{};
@@ -243,6 +414,7 @@ struct RowInitDevice {
   uint8_t *sym = nullptr, *height = nullptr;
   uint64_t *base_hr = nullptr;  // level P bases by (height, row)
   std::vector<uint64_t> base_hoff;
+  unsigned int *err = nullptr;  // set by the tensor-core product if a bounded wait gave up
   ~RowInitDevice() {
     for (void *p : allocs) cudaFree(p);
   }
@@ -348,6 +520,11 @@ cudaError_t build_device(int W, int rows, int cap, std::unique_ptr<RowInitDevice
   for (size_t i = 0; i < htop.size(); ++i) bhr[size_t(d->base_hoff[htop[i]]) + size_t(rtop[i])] = pl.base[i];
   UP(bhr, d->base_hr)
 #undef UP
+  std::vector<unsigned int> zero(1, 0u);
+  if ((e = upload(*d, zero, &d->err)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(rowinit_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMmaSmem))) !=
+      cudaSuccess)
+    return e;
   out = std::move(d);
   return cudaSuccess;
 }
@@ -381,6 +558,24 @@ cudaError_t prepare_row_init(int W, int rows, int cap) {
   return cudaSuccess;
 }
 
+int auto_row_init_rows(int W) { return W >= 18 ? 7 : (W >= 14 ? 6 : 0); }
+
+bool row_init_failed(int W, int rows, int cap) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  unsigned int *flag = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_cache.find(std::make_tuple(dev, W, rows, cap));
+    if (it == g_cache.end()) return false;
+    flag = it->second->err;
+  }
+  unsigned int h = 0;
+  if (cudaMemcpy(&h, flag, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+  if (h) cudaMemset(flag, 0, sizeof(h));
+  return h != 0;
+}
+
 uint64_t row_init_scratch(int W, int rows, int cap) {
   static std::mutex mu;
   static std::map<std::tuple<int, int, int>, uint64_t> words;
@@ -392,7 +587,8 @@ uint64_t row_init_scratch(int W, int rows, int cap) {
 }
 
 cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mods, uint32_t *main,
-                             uint32_t *scratch, uint64_t scratch_words, cudaStream_t s, uint64_t *launches) {
+                             uint32_t *scratch, uint64_t scratch_words, bool tensor, cudaStream_t s,
+                             uint64_t *launches) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -470,10 +666,18 @@ cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mo
     const uint64_t rows_h = prevA.cnt[h], cols = prevU.cnt[h];
     const int K = d->aut.K[h];
     if (!rows_h || !cols || !K) continue;
-    const uint64_t tiles = ((rows_h + TM - 1) / TM) * ((cols + TN - 1) / TN);
-    rowinit_product_kernel<<<unsigned(tiles), 256, 0, s>>>(ln, L, K, rows_h, cols, V + prevA.base[h],
-                                                           U + prevU.base[h], d->base_hr + d->base_hoff[size_t(h)],
-                                                           main);
+    if (tensor) {
+      const uint64_t items = ((rows_h + MM - 1) / MM) * ((cols + MN - 1) / MN) * uint64_t(L);
+      const uint64_t grid = std::min<uint64_t>(items, uint64_t(device_sm_count()));
+      rowinit_mma_kernel<<<unsigned(grid), 128, kMmaSmem, s>>>(ln, L, K, rows_h, cols, V + prevA.base[h],
+                                                                U + prevU.base[h],
+                                                                d->base_hr + d->base_hoff[size_t(h)], main, d->err);
+    } else {
+      const uint64_t tiles = ((rows_h + TM - 1) / TM) * ((cols + TN - 1) / TN);
+      rowinit_product_kernel<<<unsigned(tiles), 256, 0, s>>>(ln, L, K, rows_h, cols, V + prevA.base[h],
+                                                             U + prevU.base[h],
+                                                             d->base_hr + d->base_hoff[size_t(h)], main);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     ++n;
   }

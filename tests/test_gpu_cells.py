@@ -106,7 +106,7 @@ def test_tuning_never_changes_results(engine):
             assert engine.get_tuning() == {"block": block, "grid": grid, "split_panels": split,
                                            "bounded_prefix": True, "lane_items": items, "share_min": share,
                                            "compact_max_p": compact, "compact_items": citems,
-                                           "row_init_rows": 0}
+                                           "row_init_rows": 0, "row_init_product": 0}
             _run(engine, 12, 11, 1, [MODS[i % 3] for i in range(14)], seed=block + grid)
             _run(engine, 12, 3, 1, [MODS[i % 3] for i in range(8)], seed=block + items)
     finally:

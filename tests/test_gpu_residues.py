@@ -94,17 +94,20 @@ def test_bounded_prefix_equals_full_rows(engine):
         engine.set_tuning()
 
 
+@pytest.mark.parametrize("product", [0, 1], ids=["tensor-cores", "cuda-cores"])
 @pytest.mark.parametrize("rows", [2, 3, 4, 5, 6, 7])
-def test_row_init_equals_row_sweeps(engine, rows):
+def test_row_init_equals_row_sweeps(engine, rows, product):
     """The row-k initialiser (the state after the first `rows` rows of
     vertices, computed by the column automaton) gives the residues of the row
-    sweeps, in the bounded and the full space, for every lane count kind."""
+    sweeps, in the bounded and the full space, for every lane count kind, with
+    its products on the tensor cores (8-bit limbs) and on the CUDA cores."""
     try:
-        for n, mods, lanes in ((6, P[:2], 2), (9, [2, 3, P[0]], 3), (12, P[:8], 8), (14, P[:14], 14), (15, P[:3], 1)):
+        for n, mods, lanes in ((6, P[:2], 2), (9, [2, 3, P[0]], 3), (12, P[:8], 8), (14, P[:14], 14), (15, P[:3], 1),
+                               (17, [P[0], 2147483647], 2)):
             engine.set_tuning(row_init_rows=-1)
             want = engine.residues(n, mods, lanes=lanes).residues
             for bounded in (True, False):
-                engine.set_tuning(bounded_prefix=bounded, row_init_rows=rows)
+                engine.set_tuning(bounded_prefix=bounded, row_init_rows=rows, row_init_product=product)
                 assert engine.residues(n, mods, lanes=lanes).residues == want, (n, rows, bounded)
     finally:
         engine.set_tuning()

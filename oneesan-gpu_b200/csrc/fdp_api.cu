@@ -57,6 +57,8 @@ static fdp_status check_problem(const fdp_problem *pr) {
   return FDP_OK;
 }
 
+static int fit_row_init(int W, int R, bool bounded, int *cap);
+
 extern "C" fdp_status fdp_plan(const fdp_problem *pr, uint64_t budget, fdp_plan_out *out) {
   fdp_status s = check_problem(pr);
   if (s != FDP_OK) return s;
@@ -84,12 +86,8 @@ extern "C" fdp_status fdp_plan(const fdp_problem *pr, uint64_t budget, fdp_plan_
   // (default tuning, when its scratch fits).
   std::vector<int> caps;
   if (W >= 4) caps = fdp::bounded_prefix_caps(W);
-  int R = fdp::auto_row_init_rows(W);
-  if (R > W - 1) R = W - 1;
-  if (R >= 2) {
-    const int cap = R <= int(caps.size()) ? caps[size_t(R - 1)] : FDP_FULL_CAP;
-    if (fdp::row_init_scratch(W, R, cap) > fdp::blocked_states(W)) R = 0;
-  }
+  int R = fdp::auto_row_init_rows(W), rcap = 0;
+  if (R >= 2) R = fit_row_init(W, R, true, &rcap);
   o.init_rows = R;
   const int first_row = R >= 2 ? R : 1;
   o.bounded_rows = 0;
@@ -174,17 +172,23 @@ fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const DevTables **out) {
 // starts from row 0), and the height cap of the space row R runs in.  Used
 // when the fill's scratch fits the blocked buffer (D words per lane, dead
 // before the first sweep).
+// The largest strip of at most R rows whose fill fits the blocked buffer.
+static int fit_row_init(int W, int R, bool bounded, int *cap) {
+  if (R > W - 1) R = W - 1;  // the state after row R-1 <= the last sweep row
+  if (R > 7) R = 7;
+  const std::vector<int> caps = (bounded && W >= 4) ? fdp::bounded_prefix_caps(W) : std::vector<int>{};
+  for (; R >= 2; --R) {
+    *cap = R <= int(caps.size()) ? caps[size_t(R - 1)] : FDP_FULL_CAP;
+    if (fdp::row_init_scratch(W, R, *cap) <= fdp::blocked_states(W)) return R;
+  }
+  return 0;
+}
+
 static int row_init_rows(const fdp_ctx *c, int W, int *cap) {
   int R = c->cfg.row_init;
   if (R == 0) R = fdp::auto_row_init_rows(W);
   if (R < 2) return 0;
-  if (R > W - 1) R = W - 1;         // the state after row R-1 <= the last sweep row
-  if (R > 7) R = 7;
-  if (R < 2) return 0;
-  const std::vector<int> caps = (c->cfg.bounded_prefix && W >= 4) ? fdp::bounded_prefix_caps(W) : std::vector<int>{};
-  *cap = R <= int(caps.size()) ? caps[size_t(R - 1)] : FDP_FULL_CAP;
-  if (fdp::row_init_scratch(W, R, *cap) > fdp::blocked_states(W)) return 0;
-  return R;
+  return fit_row_init(W, R, c->cfg.bounded_prefix, cap);
 }
 
 // Every device table a residue pass of width W reads, uploaded before any

@@ -399,7 +399,16 @@ uint64_t row_init_scratch_words(const RowInitPlan &pl) {
     for (int g = 0; g <= pl.hmax; ++g) w += pl.C[size_t(k)][size_t(g)] * uint64_t(pl.K[size_t(g)]);
     suf = std::max(suf, w);
   }
-  return 2 * pre + 2 * suf;
+  // The tensor-core product's packed limb tiles of one height at a time:
+  // 128-row A tiles of 16 KB and 64-row B tiles of 8 KB per 32-wide K step.
+  uint64_t packed = 0;
+  for (int h = 0; h <= pl.hmax; ++h) {
+    const uint64_t K = uint64_t(pl.K[size_t(h)]), nks = (K + 31) / 32;
+    const uint64_t rows = pl.rows_of[size_t(pl.P - 1)][size_t(h)], cols = pl.C[size_t(pl.S)][size_t(h)];
+    if (!K || !rows || !cols) continue;
+    packed = std::max(packed, ((rows + 127) / 128) * nks * 4096 + ((cols + 63) / 64) * nks * 2048);
+  }
+  return 2 * ((pre + 3) & ~uint64_t(3)) + 2 * ((suf + 3) & ~uint64_t(3)) + packed;
 }
 
 std::vector<uint32_t> row_init_fill_host(const RowInitPlan &pl, uint32_t mod) {

@@ -33,6 +33,7 @@ struct Lanes {
   unsigned long long m[16];  // floor((2^64 - 1) / p)
   uint64_t off[16];          // word offset of lane l's panel: L0 * N + (l - L0)
   int pw[16];                // panel width of lane l
+  uint32_t c8[16][7];        // 2^(8s) mod p, s = 0..6 (tensor-core product's limb shifts)
 };
 
 __device__ __forceinline__ uint32_t red64(unsigned long long x, uint32_t p, unsigned long long m) {
@@ -237,19 +238,33 @@ __global__ void __launch_bounds__(256) rowinit_product_kernel(Lanes ln, int L, i
 // Every value is split into four u8 limbs, v = sum_i 2^(8i) v_i; the 16 limb
 // products accumulate by shift s = i + j into seven s32 accumulators in tensor
 // memory (7 x 64 of the 512 columns), so out = sum_s 2^(8s) G_s mod p.  A
-// group sums at most 4 x K x 255^2 < 2^31 for K <= 8192.  Tiles of 128
-// prefixes x 64 completions, K in steps of 32 bytes; each thread splits its
-// row's values into the limbs' shared-memory tiles (K-major, no swizzle:
-// core matrices of 8 rows x 16 bytes, 256 bytes between 8-row groups, 128
-// bytes between the two 16-byte K halves), one thread issues the MMAs and
-// commits them to an mbarrier that every thread waits on (bounded).  One CTA
-// per SM (it holds all 512 tensor-memory columns), persistent over
-// (tile, lane) items; all lanes of a tile run back to back.
+// group sums at most 4 x K x 255^2 < 2^28 for K <= 1024 (larger K uses the
+// CUDA-core product), so sum_s G_s (2^(8s) mod p) fits 64 bits and each output
+// needs one reduction.
+//
+// Operands are first packed (rowinit_pack_kernel) into the tensor cores'
+// shared-memory layout, one contiguous tile per 32-wide K step: K-major, no
+// swizzle, core matrices of 8 rows x 16 bytes, 256 bytes between 8-row
+// groups, 128 bytes between the two 16-byte K halves, the four limbs one after
+// the other (128-row A tiles of 16 KB, 64-row B tiles of 8 KB).  The product
+// kernel then streams them with bulk copies into an 8-stage ring: thread 0
+// issues the copies (each stage completes an mbarrier by bytes), the MMAs of a
+// stage as soon as it has landed, and commits them to the stage's "empty"
+// mbarrier, so the copies of the next stages overlap the MMAs.  After an
+// item's last step it commits to an accumulator barrier; all eight warps then
+// read tensor memory (warps w and w+4: rows 32w..32w+31, one half of the
+// columns each) and recombine the limbs mod p while the next item's copies are
+// already in flight.  Every wait is bounded.  One
+// CTA per SM (it holds all 512 tensor-memory columns), persistent over
+// (tile, lane) items, lanes innermost so a state's panel words are written
+// close together in time.
 constexpr int MM = 128, MN = 64, MK = 32;
-constexpr int A_LIMB = MM * MK, B_LIMB = MN * MK;  // bytes of one limb's tile per K step
+constexpr int A_LIMB = MM * MK, B_LIMB = MN * MK;         // bytes of one limb's tile per K step
+constexpr int A_TILE = 4 * A_LIMB, B_TILE = 4 * B_LIMB;   // 16 KB, 8 KB
+constexpr int NST = 8;                                    // ring stages
 constexpr uint32_t kIdescI8 = (2u << 4) | (uint32_t(MN >> 3) << 17) | (uint32_t(MM >> 4) << 24);  // S32 += U8 x U8, K-major
 constexpr uint32_t kTmemCols = 512;
-constexpr size_t kMmaSmem = 120 * 1024;  // more than half an SM's shared memory: one CTA per SM
+constexpr size_t kMmaSmem = NST * (A_TILE + B_TILE);  // the ring: 192 KB, so one CTA per SM
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
 
@@ -273,39 +288,60 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
   return false;
 }
 
-// Row `row` of a 128- or 64-row operand tile: 32 values -> 4 limb tiles.
-__device__ __forceinline__ void stage_row(unsigned char *tile, int limb_bytes, int row, const uint32_t *src, int k0,
-                                          int K, bool valid) {
-  uint32_t v[MK];
+// Pack rows of a K-contiguous operand (count rows x K per lane, lane stride
+// count x K) into limb tiles of `rows_per_tile` rows: tile (lane, block, step)
+// at ((lane x blocks + block) x steps + step) x tile_bytes.
+__global__ void __launch_bounds__(256) rowinit_pack_kernel(const uint32_t *src, uint64_t count, int K, int L,
+                                                           int rows_per_tile, unsigned char *dst) {
+  const int steps = (K + MK - 1) / MK;
+  const uint64_t blocks = (count + rows_per_tile - 1) / rows_per_tile;
+  const int limb_bytes = rows_per_tile * MK, tile_bytes = 4 * limb_bytes;
+  const uint64_t total = uint64_t(L) * blocks * uint64_t(rows_per_tile) * uint64_t(steps);
+  for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < total; w += uint64_t(gridDim.x) * blockDim.x) {
+    const int ks = int(w % uint64_t(steps));
+    uint64_t rest = w / uint64_t(steps);
+    const int r = int(rest % uint64_t(rows_per_tile));
+    rest /= uint64_t(rows_per_tile);
+    const uint64_t blk = rest % blocks, l = rest / blocks;
+    const uint64_t row = blk * uint64_t(rows_per_tile) + uint64_t(r);
+    const uint32_t *rp = src + (l * count + row) * uint64_t(K);
+    uint32_t v[MK];
 #pragma unroll
-  for (int k = 0; k < MK; ++k) v[k] = (valid && k0 + k < K) ? src[k0 + k] : 0u;
-  const int roff = (row >> 3) * 256 + (row & 7) * 16;
+    for (int k = 0; k < MK; ++k) v[k] = (row < count && ks * MK + k < K) ? rp[ks * MK + k] : 0u;
+    unsigned char *tile = dst + ((l * blocks + blk) * uint64_t(steps) + uint64_t(ks)) * uint64_t(tile_bytes);
+    const int roff = (r >> 3) * 256 + (r & 7) * 16;
 #pragma unroll
-  for (int limb = 0; limb < 4; ++limb) {
-    const int sh = 8 * limb;
+    for (int limb = 0; limb < 4; ++limb) {
+      const int sh = 8 * limb;
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      uint32_t w[4];
+      for (int c = 0; c < 2; ++c) {
+        uint32_t q4[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int k = c * 16 + q * 4;
-        w[q] = ((v[k] >> sh) & 0xffu) | (((v[k + 1] >> sh) & 0xffu) << 8) | (((v[k + 2] >> sh) & 0xffu) << 16) |
-               (((v[k + 3] >> sh) & 0xffu) << 24);
+        for (int q = 0; q < 4; ++q) {
+          const int k = c * 16 + q * 4;
+          q4[q] = ((v[k] >> sh) & 0xffu) | (((v[k + 1] >> sh) & 0xffu) << 8) | (((v[k + 2] >> sh) & 0xffu) << 16) |
+                  (((v[k + 3] >> sh) & 0xffu) << 24);
+        }
+        *reinterpret_cast<uint4 *>(tile + limb * limb_bytes + roff + c * 128) = make_uint4(q4[0], q4[1], q4[2], q4[3]);
       }
-      *reinterpret_cast<uint4 *>(tile + limb * limb_bytes + roff + c * 128) = make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
 }
 
-__global__ void __launch_bounds__(128, 1) rowinit_mma_kernel(Lanes ln, int L, int K, uint64_t n, uint64_t C,
-                                                             const uint32_t *V, const uint32_t *U,
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int L, int K, uint64_t n, uint64_t C,
+                                                             const unsigned char *Ap, const unsigned char *Bp,
                                                              const uint64_t *base, uint32_t *out,
                                                              unsigned int *err) {
   extern __shared__ __align__(1024) unsigned char dsm[];
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t full_bar[NST], empty_bar[NST], acc_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
-  unsigned char *sA = dsm, *sB = dsm + 4 * A_LIMB;
   const int t = threadIdx.x, warp = t >> 5;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
@@ -314,40 +350,72 @@ __global__ void __launch_bounds__(128, 1) rowinit_mma_kernel(Lanes ln, int L, in
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (t == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1) : "memory");
+    for (int i = 0; i < NST; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full_bar[i])), "r"(1) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty_bar[i])), "r"(1) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&acc_bar)), "r"(1) : "memory");
     abort_flag = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t tmem = tmem_slot, bar = smem_addr(&mbar);
-  uint32_t phase = 0;
-  const uint64_t tiles_n = (C + MN - 1) / MN, tiles = ((n + MM - 1) / MM) * tiles_n;
-  const uint64_t items = tiles * uint64_t(L);
+  const uint32_t tmem = tmem_slot;
   const int nks = (K + MK - 1) / MK;
-  for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
+  const uint64_t rblocks = (n + MM - 1) / MM, cblocks = (C + MN - 1) / MN;
+  const uint64_t items = rblocks * cblocks * uint64_t(L);
+  const uint64_t my_items = items > blockIdx.x ? (items - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  const uint64_t steps = my_items * uint64_t(nks);  // this CTA's K steps, in order
+  // Step g of this CTA: its item, lane, tile and K step.
+  auto decode = [&](uint64_t g, uint64_t &rb, uint64_t &cb, int &l, int &ks) {
+    const uint64_t it = blockIdx.x + (g / uint64_t(nks)) * gridDim.x;
+    ks = int(g % uint64_t(nks));
+    l = int(it % uint64_t(L));
     const uint64_t tile = it / uint64_t(L);
-    const int l = int(it % uint64_t(L));
-    const uint64_t i0 = (tile / tiles_n) * MM, j0 = (tile % tiles_n) * MN;
-    const uint32_t *Vl = V + uint64_t(l) * n * uint64_t(K), *Ul = U + uint64_t(l) * C * uint64_t(K);
-    const uint64_t gi = i0 + uint64_t(t);
-    for (int ks = 0; ks < nks; ++ks) {
-      stage_row(sA, A_LIMB, t, Vl + (gi < n ? gi : 0) * uint64_t(K), ks * MK, K, gi < n);
-      if (t < MN) {
-        const uint64_t gj = j0 + uint64_t(t);
-        stage_row(sB, B_LIMB, t, Ul + (gj < C ? gj : 0) * uint64_t(K), ks * MK, K, gj < C);
+    cb = tile % cblocks;
+    rb = tile / cblocks;
+  };
+  uint64_t issued = 0;  // steps whose copies were issued (thread 0)
+  auto issue_copy = [&](uint64_t g) -> bool {
+    const int s = int(g % NST);
+    const uint64_t use = g / NST;
+    if (use > 0 && !mbar_wait(smem_addr(&empty_bar[s]), uint32_t((use - 1) & 1u))) return false;
+    uint64_t rb, cb;
+    int l, ks;
+    decode(g, rb, cb, l, ks);
+    const unsigned char *a = Ap + ((uint64_t(l) * rblocks + rb) * uint64_t(nks) + uint64_t(ks)) * uint64_t(A_TILE);
+    const unsigned char *b = Bp + ((uint64_t(l) * cblocks + cb) * uint64_t(nks) + uint64_t(ks)) * uint64_t(B_TILE);
+    const uint32_t fb = smem_addr(&full_bar[s]);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(uint32_t(A_TILE + B_TILE)), "r"(fb)
+                 : "memory");
+    unsigned char *st = dsm + size_t(s) * (A_TILE + B_TILE);
+    bulk_load(smem_addr(st), a, A_TILE, fb);
+    bulk_load(smem_addr(st + A_TILE), b, B_TILE, fb);
+    return true;
+  };
+  uint64_t g = 0;
+  for (uint64_t item = 0; item < my_items; ++item) {
+    if (t == 0) {
+      // Keep NST - 1 steps of copies ahead of the MMAs.
+      while (issued < steps && issued < g + NST - 1 && !abort_flag) {
+        if (!issue_copy(issued)) abort_flag = 1;
+        ++issued;
       }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncthreads();
-      if (t == 0) {
+      for (int ks = 0; ks < nks && !abort_flag; ++ks, ++g) {
+        const int s = int(g % NST);
+        if (!mbar_wait(smem_addr(&full_bar[s]), uint32_t((g / NST) & 1u))) {
+          abort_flag = 1;
+          break;
+        }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned char *st = dsm + size_t(s) * (A_TILE + B_TILE);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             const int sft = i + j;
             const uint32_t en = (ks > 0 || i != (sft > 3 ? sft - 3 : 0)) ? 1u : 0u;
-            const uint64_t da = umma_desc(smem_addr(sA + i * A_LIMB)), db = umma_desc(smem_addr(sB + j * B_LIMB));
+            const uint64_t da = umma_desc(smem_addr(st + i * A_LIMB)), db = umma_desc(smem_addr(st + A_TILE + j * B_LIMB));
             asm volatile(
                 "{\n\t.reg .pred PRED_enable_input_d;\n\t"
                 "setp.ne.b32 PRED_enable_input_d, %4, 0;\n\t"
@@ -356,37 +424,60 @@ __global__ void __launch_bounds__(128, 1) rowinit_mma_kernel(Lanes ln, int L, in
                 : "r"(tmem + uint32_t(sft * MN)), "l"(da), "l"(db), "r"(kIdescI8), "r"(en)
                 : "memory");
           }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&empty_bar[s]))
                      : "memory");
+        // Refill the stage of step g - 1 (its MMAs were issued before these
+        // ones) with step g + NST - 1 while this step's MMAs run.
+        if (issued < steps && issued == g + NST - 1) {
+          if (!issue_copy(issued)) {
+            abort_flag = 1;
+            break;
+          }
+          ++issued;
+        }
       }
-      // The MMAs read the staged tiles: wait for them before the next stage.
-      if (!mbar_wait(bar, phase)) atomicExch(&abort_flag, 1);
-      phase ^= 1u;
-      __syncthreads();
-      if (abort_flag) break;
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_addr(&acc_bar))
+                   : "memory");
     }
+    // The item's accumulators are complete.
+    if (!mbar_wait(smem_addr(&acc_bar), uint32_t(item & 1u))) abort_flag = 1;
+    __syncthreads();
     if (abort_flag) break;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // Rows 32w..32w+31 of the tile are tensor-memory lanes of warp w.
+    uint64_t rb, cb;
+    int l, ks0;
+    decode(item * uint64_t(nks), rb, cb, l, ks0);
+    // Warp w reads tensor-memory lanes 32 (w mod 4) .. + 31 (the tile's rows)
+    // and columns 32 (w / 4) .. + 31.  G_s < 4 K 255^2 < 2^28 (K <= 1024), so
+    // sum_s G_s (2^(8s) mod p) < 7 x 2^60 fits 64 bits: one reduction per output.
+    const int quarter = warp & 3, half = warp >> 2;
+    const uint64_t gi = rb * MM + uint64_t(quarter * 32 + (t & 31)), j0 = cb * MN;
     const uint32_t p = ln.p[l];
     const unsigned long long m = ln.m[l];
     const uint64_t b0 = gi < n ? base[gi] : 0;
-    for (int c = 0; c < MN; c += 16) {
+    for (int c = half * 32; c < half * 32 + 32; c += 16) {
       unsigned long long acc[16];
 #pragma unroll
       for (int q = 0; q < 16; ++q) acc[q] = 0;
-      for (int sft = 6; sft >= 0; --sft) {
-        uint32_t g[16];
+#pragma unroll
+      for (int sft = 0; sft < 7; ++sft) {
+        uint32_t gv[16];
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
             "%14, %15}, [%16];"
-            : "=r"(g[0]), "=r"(g[1]), "=r"(g[2]), "=r"(g[3]), "=r"(g[4]), "=r"(g[5]), "=r"(g[6]), "=r"(g[7]),
-              "=r"(g[8]), "=r"(g[9]), "=r"(g[10]), "=r"(g[11]), "=r"(g[12]), "=r"(g[13]), "=r"(g[14]), "=r"(g[15])
-            : "r"(tmem + (uint32_t(warp * 32) << 16) + uint32_t(sft * MN + c)));
+            : "=r"(gv[0]), "=r"(gv[1]), "=r"(gv[2]), "=r"(gv[3]), "=r"(gv[4]), "=r"(gv[5]), "=r"(gv[6]), "=r"(gv[7]),
+              "=r"(gv[8]), "=r"(gv[9]), "=r"(gv[10]), "=r"(gv[11]), "=r"(gv[12]), "=r"(gv[13]), "=r"(gv[14]),
+              "=r"(gv[15])
+            : "r"(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(sft * MN + c)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const uint32_t cs = ln.c8[l][sft];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = red64(acc[q] * 256ull + g[q], p, m);
+        for (int q = 0; q < 16; ++q) acc[q] += (unsigned long long)gv[q] * cs;
       }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc[q] = red64(acc[q], p, m);
       if (gi < n) {
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
@@ -614,6 +705,11 @@ cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mo
   for (int l = 0; l < L; ++l) {
     ln.p[l] = mods[l];
     ln.m[l] = ~0ull / mods[l];
+    uint64_t c = 1 % mods[l];
+    for (int sft = 0; sft < 7; ++sft) {
+      ln.c8[l][sft] = uint32_t(c);
+      c = (c << 8) % mods[l];
+    }
   }
   uint64_t pre_words = 0, suf_words = 0;
   for (int k = 0; k < pl.P; ++k) {
@@ -626,6 +722,8 @@ cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mo
     for (int g = 0; g <= pl.hmax; ++g) w += pl.C[size_t(k)][size_t(g)] * uint64_t(pl.K[size_t(g)]);
     suf_words = std::max(suf_words, w * uint64_t(L));
   }
+  pre_words = (pre_words + 3) & ~uint64_t(3);
+  suf_words = (suf_words + 3) & ~uint64_t(3);
   uint32_t *pre[2] = {scratch, scratch + pre_words};
   uint32_t *suf[2] = {scratch + 2 * pre_words, scratch + 2 * pre_words + suf_words};
   if ((e = cudaMemsetAsync(main, 0, size_t(pl.states) * L * 4, s)) != cudaSuccess) return e;
@@ -666,11 +764,19 @@ cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mo
     const uint64_t rows_h = prevA.cnt[h], cols = prevU.cnt[h];
     const int K = d->aut.K[h];
     if (!rows_h || !cols || !K) continue;
-    if (tensor) {
-      const uint64_t items = ((rows_h + MM - 1) / MM) * ((cols + MN - 1) / MN) * uint64_t(L);
+    if (tensor && K <= 1024) {
+      // Packed limb tiles after the level buffers (16-byte aligned).
+      unsigned char *ap = reinterpret_cast<unsigned char *>(scratch + 2 * pre_words + 2 * suf_words);
+      const uint64_t nks = uint64_t(K + MK - 1) / MK, rblocks = (rows_h + MM - 1) / MM, cblocks = (cols + MN - 1) / MN;
+      unsigned char *bp = ap + uint64_t(L) * rblocks * nks * A_TILE;
+      const int pblocks = device_sm_count() * 8;
+      rowinit_pack_kernel<<<pblocks, 256, 0, s>>>(V + prevA.base[h], rows_h, K, L, MM, ap);
+      rowinit_pack_kernel<<<pblocks, 256, 0, s>>>(U + prevU.base[h], cols, K, L, MN, bp);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      n += 2;
+      const uint64_t items = rblocks * cblocks * uint64_t(L);
       const uint64_t grid = std::min<uint64_t>(items, uint64_t(device_sm_count()));
-      rowinit_mma_kernel<<<unsigned(grid), 128, kMmaSmem, s>>>(ln, L, K, rows_h, cols, V + prevA.base[h],
-                                                                U + prevU.base[h],
+      rowinit_mma_kernel<<<unsigned(grid), 256, kMmaSmem, s>>>(ln, L, K, rows_h, cols, ap, bp,
                                                                 d->base_hr + d->base_hoff[size_t(h)], main, d->err);
     } else {
       const uint64_t tiles = ((rows_h + TM - 1) / TM) * ((cols + TN - 1) / TN);

@@ -251,10 +251,10 @@ __global__ void __launch_bounds__(256) rowinit_product_kernel(Lanes ln, int L, i
 // issues the copies (each stage completes an mbarrier by bytes), the MMAs of a
 // stage as soon as it has landed, and commits them to the stage's "empty"
 // mbarrier, so the copies of the next stages overlap the MMAs.  After an
-// item's last step it commits to an accumulator barrier; all eight warps then
-// read tensor memory (warps w and w+4: rows 32w..32w+31, one half of the
-// columns each) and recombine the limbs mod p while the next item's copies are
-// already in flight.  Every wait is bounded.  One
+// item's last step it commits to an accumulator barrier.  Warps 4..7 then read
+// the seven groups of their rows out of tensor memory into register sums,
+// hand tensor memory back (an mbarrier the issuer waits on before the next
+// item's MMAs), and reduce mod p and store while those MMAs run.  Every wait is bounded.  One
 // CTA per SM (it holds all 512 tensor-memory columns), persistent over
 // (tile, lane) items, lanes innermost so a state's panel words are written
 // close together in time.
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int L, in
                                                              const uint64_t *base, uint32_t *out,
                                                              unsigned int *err) {
   extern __shared__ __align__(1024) unsigned char dsm[];
-  __shared__ __align__(8) uint64_t full_bar[NST], empty_bar[NST], acc_bar;
+  __shared__ __align__(8) uint64_t full_bar[NST], empty_bar[NST], acc_full, acc_empty;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   const int t = threadIdx.x, warp = t >> 5;
@@ -354,7 +354,8 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int L, in
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full_bar[i])), "r"(1) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty_bar[i])), "r"(1) : "memory");
     }
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&acc_bar)), "r"(1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&acc_full)), "r"(1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&acc_empty)), "r"(128) : "memory");
     abort_flag = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -375,33 +376,43 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int L, in
     cb = tile % cblocks;
     rb = tile / cblocks;
   };
-  uint64_t issued = 0;  // steps whose copies were issued (thread 0)
-  auto issue_copy = [&](uint64_t g) -> bool {
-    const int s = int(g % NST);
-    const uint64_t use = g / NST;
-    if (use > 0 && !mbar_wait(smem_addr(&empty_bar[s]), uint32_t((use - 1) & 1u))) return false;
-    uint64_t rb, cb;
-    int l, ks;
-    decode(g, rb, cb, l, ks);
-    const unsigned char *a = Ap + ((uint64_t(l) * rblocks + rb) * uint64_t(nks) + uint64_t(ks)) * uint64_t(A_TILE);
-    const unsigned char *b = Bp + ((uint64_t(l) * cblocks + cb) * uint64_t(nks) + uint64_t(ks)) * uint64_t(B_TILE);
-    const uint32_t fb = smem_addr(&full_bar[s]);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(uint32_t(A_TILE + B_TILE)), "r"(fb)
-                 : "memory");
-    unsigned char *st = dsm + size_t(s) * (A_TILE + B_TILE);
-    bulk_load(smem_addr(st), a, A_TILE, fb);
-    bulk_load(smem_addr(st + A_TILE), b, B_TILE, fb);
-    return true;
-  };
-  uint64_t g = 0;
-  for (uint64_t item = 0; item < my_items; ++item) {
-    if (t == 0) {
-      // Keep NST - 1 steps of copies ahead of the MMAs.
-      while (issued < steps && issued < g + NST - 1 && !abort_flag) {
-        if (!issue_copy(issued)) abort_flag = 1;
+  if (t == 0) {
+    // Producer and MMA issuer: copies run NST - 1 steps ahead of the MMAs;
+    // an item's MMAs start once the epilogue has read the previous item's
+    // accumulators out of tensor memory.
+    uint64_t issued = 0, g = 0;
+    auto issue_copy = [&](uint64_t q) -> bool {
+      const int s = int(q % NST);
+      const uint64_t use = q / NST;
+      if (use > 0 && !mbar_wait(smem_addr(&empty_bar[s]), uint32_t((use - 1) & 1u))) return false;
+      uint64_t rb, cb;
+      int l, ks;
+      decode(q, rb, cb, l, ks);
+      const unsigned char *a = Ap + ((uint64_t(l) * rblocks + rb) * uint64_t(nks) + uint64_t(ks)) * uint64_t(A_TILE);
+      const unsigned char *b = Bp + ((uint64_t(l) * cblocks + cb) * uint64_t(nks) + uint64_t(ks)) * uint64_t(B_TILE);
+      const uint32_t fb = smem_addr(&full_bar[s]);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(uint32_t(A_TILE + B_TILE)), "r"(fb)
+                   : "memory");
+      unsigned char *st = dsm + size_t(s) * (A_TILE + B_TILE);
+      bulk_load(smem_addr(st), a, A_TILE, fb);
+      bulk_load(smem_addr(st + A_TILE), b, B_TILE, fb);
+      return true;
+    };
+    for (uint64_t item = 0; item < my_items && !abort_flag; ++item) {
+      while (issued < steps && issued < g + NST - 1) {
+        if (!issue_copy(issued)) {
+          abort_flag = 1;
+          break;
+        }
         ++issued;
       }
-      for (int ks = 0; ks < nks && !abort_flag; ++ks, ++g) {
+      if (abort_flag) break;
+      if (item > 0 && !mbar_wait(smem_addr(&acc_empty), uint32_t((item - 1) & 1u))) {
+        abort_flag = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int ks = 0; ks < nks; ++ks, ++g) {
         const int s = int(g % NST);
         if (!mbar_wait(smem_addr(&full_bar[s]), uint32_t((g / NST) & 1u))) {
           abort_flag = 1;
@@ -437,58 +448,65 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int L, in
           ++issued;
         }
       }
+      // The item's accumulators are complete once its MMAs are.
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_addr(&acc_bar))
+                       smem_addr(&acc_full))
                    : "memory");
     }
-    // The item's accumulators are complete.
-    if (!mbar_wait(smem_addr(&acc_bar), uint32_t(item & 1u))) abort_flag = 1;
-    __syncthreads();
-    if (abort_flag) break;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    uint64_t rb, cb;
-    int l, ks0;
-    decode(item * uint64_t(nks), rb, cb, l, ks0);
-    // Warp w reads tensor-memory lanes 32 (w mod 4) .. + 31 (the tile's rows)
-    // and columns 32 (w / 4) .. + 31.  G_s < 4 K 255^2 < 2^28 (K <= 1024), so
-    // sum_s G_s (2^(8s) mod p) < 7 x 2^60 fits 64 bits: one reduction per output.
-    const int quarter = warp & 3, half = warp >> 2;
-    const uint64_t gi = rb * MM + uint64_t(quarter * 32 + (t & 31)), j0 = cb * MN;
-    const uint32_t p = ln.p[l];
-    const unsigned long long m = ln.m[l];
-    const uint64_t b0 = gi < n ? base[gi] : 0;
-    for (int c = half * 32; c < half * 32 + 32; c += 16) {
-      unsigned long long acc[16];
-#pragma unroll
-      for (int q = 0; q < 16; ++q) acc[q] = 0;
-#pragma unroll
-      for (int sft = 0; sft < 7; ++sft) {
-        uint32_t gv[16];
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-            "%14, %15}, [%16];"
-            : "=r"(gv[0]), "=r"(gv[1]), "=r"(gv[2]), "=r"(gv[3]), "=r"(gv[4]), "=r"(gv[5]), "=r"(gv[6]), "=r"(gv[7]),
-              "=r"(gv[8]), "=r"(gv[9]), "=r"(gv[10]), "=r"(gv[11]), "=r"(gv[12]), "=r"(gv[13]), "=r"(gv[14]),
-              "=r"(gv[15])
-            : "r"(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(sft * MN + c)));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        const uint32_t cs = ln.c8[l][sft];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] += (unsigned long long)gv[q] * cs;
+  } else if (warp >= 4) {
+    // Epilogue warps 4..7: warp w reads tensor-memory lanes 32 (w - 4) .. + 31
+    // (the tile's rows), sums the limb groups of its row's 64 outputs into
+    // registers, hands tensor memory back, then reduces and stores while the
+    // next item's MMAs run.  G_s < 4 K 255^2 < 2^28 (K <= 1024), so
+    // sum_s G_s (2^(8s) mod p) < 7 x 2^60 fits 64 bits.
+    const int quarter = warp - 4;
+    for (uint64_t item = 0; item < my_items; ++item) {
+      if (!mbar_wait(smem_addr(&acc_full), uint32_t(item & 1u))) {
+        abort_flag = 1;
+        break;
       }
+      if (abort_flag) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint64_t rb, cb;
+      int l, ks0;
+      decode(item * uint64_t(nks), rb, cb, l, ks0);
+      unsigned long long acc[MN];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) acc[q] = red64(acc[q], p, m);
+      for (int q = 0; q < MN; ++q) acc[q] = 0;
+#pragma unroll
+      for (int c = 0; c < MN; c += 16) {
+#pragma unroll
+        for (int sft = 0; sft < 7; ++sft) {
+          uint32_t gv[16];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+              "%14, %15}, [%16];"
+              : "=r"(gv[0]), "=r"(gv[1]), "=r"(gv[2]), "=r"(gv[3]), "=r"(gv[4]), "=r"(gv[5]), "=r"(gv[6]),
+                "=r"(gv[7]), "=r"(gv[8]), "=r"(gv[9]), "=r"(gv[10]), "=r"(gv[11]), "=r"(gv[12]), "=r"(gv[13]),
+                "=r"(gv[14]), "=r"(gv[15])
+              : "r"(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(sft * MN + c)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          const uint32_t cs = ln.c8[l][sft];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) acc[c + q] += (unsigned long long)gv[q] * cs;
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&acc_empty)) : "memory");
+      const uint64_t gi = rb * MM + uint64_t(quarter * 32 + (t & 31)), j0 = cb * MN;
       if (gi < n) {
+        const uint32_t p = ln.p[l];
+        const unsigned long long m = ln.m[l];
+        const uint64_t b0 = base[gi];
+        uint32_t *o = out + ln.off[l];
+        const uint64_t pw = uint64_t(ln.pw[l]);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const uint64_t gj = j0 + uint64_t(c + q);
-          if (gj < C) out[ln.off[l] + (b0 + gj) * uint64_t(ln.pw[l])] = uint32_t(acc[q]);
+        for (int q = 0; q < MN; ++q) {
+          const uint64_t gj = j0 + uint64_t(q);
+          if (gj < C) o[(b0 + gj) * pw] = red64(acc[q], p, m);
         }
       }
     }
-    // Every read of the accumulators is done before the next item's MMAs.
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
   }
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");

@@ -94,8 +94,10 @@ extern "C" fdp_status fdp_autotune(fdp_ctx *c, const fdp_problem *pr, uint64_t b
         }
         const double row = median(samples);
         const int passes = (k + L - 1) / L;
-        // Each pass runs `rows` sweeps; spread over the k residues.
-        const double spr = row * 1e-3 * rows * passes / k;
+        // Each pass sweeps the rows the row-k initialiser does not fill
+        // (its own fill is left out of the estimate); spread over k residues.
+        const int swept = rows - (plan.init_rows >= 2 ? plan.init_rows - 1 : 0);
+        const double spr = row * 1e-3 * swept * passes / k;
         snprintf(buf, sizeof(buf),
                  "%s{\"lanes\":%d,\"split_panels\":%d,\"block\":%d,\"status\":\"ok\",\"row_ms\":%.4f,"
                  "\"s_per_residue\":%.6f,\"passes\":%d}",

@@ -7,8 +7,10 @@ import fcntl
 import hashlib
 import json
 import os
+import signal
 import subprocess
 import sys
+import time
 
 import pytest
 
@@ -33,6 +35,8 @@ for i, p in enumerate(mods):
     if mode == "big": r = p + 1
     if mode == "corrupt" and i == 0: r = (r + 1) % p
     if mode == "stop" and i == 1: sys.exit(3)
+    if mode == "slow" and i == 1:
+        import time; time.sleep(120)
     wall = "0.25"
     if mode == "walls": wall = ["1e-05", "0.1", "123456789012.5", "1e+16", "2.5e-07", "3.141592653589793", "0"][i % 7]
     print(f"backend=fake n={{n}} residue={{r}} modulus={{p}} extra=1 wall_s={{wall}}", flush=True)
@@ -200,3 +204,47 @@ def test_in_process_exact_count_on_gpu(tmp_path):
     assert f"exact={COUNTS[9]}" in r.stdout
     ck = json.loads((tmp_path / "w" / "checkpoint.json").read_text())
     assert ck["solver"]["binary_name"] == "libfdp.so"
+
+
+def test_solver_crash_then_resume(tmp_path):
+    # The solver dies after its first residue: the driver fails, but the
+    # residue it had already reported is in the durable checkpoint, and the
+    # next run asks only for the rest and finishes with the exact count.
+    solver = fake_solver(tmp_path)
+    r = run(9, tmp_path / "w", solver, mode="stop")
+    assert r.returncode == 1 and "rc=3" in r.stderr
+    ck = json.loads((tmp_path / "w" / "checkpoint.json").read_text())
+    assert list(ck["residues"]) == ["4294967291"]
+    r = run(9, tmp_path / "w", solver)
+    assert r.returncode == 0 and f"exact={COUNTS[9]}" in r.stdout
+    man = json.loads((tmp_path / "w" / "exact_manifest.json").read_text())
+    ck = json.loads((tmp_path / "w" / "checkpoint.json").read_text())
+    assert man["exact_decimal"] == str(COUNTS[9])
+    assert len(man["congruences"]) == len(ck["residues"]) == man["primes_used"]
+
+
+def test_driver_killed_then_resume(tmp_path):
+    # The driver (and its solver) are killed while a batch is in flight; the
+    # checkpoint on disk stays a valid V4 file, the work-directory lock dies
+    # with the process, and a new run resumes and finishes.
+    solver = fake_solver(tmp_path)
+    work = tmp_path / "w"
+    env = dict(os.environ, FAKE_EXACT=str(COUNTS[9]), FAKE_MODE="slow")
+    p = subprocess.Popen([EXACT, "9", "--work-dir", str(work), "--binary", solver], env=env,
+                         stdout=subprocess.PIPE, stderr=subprocess.PIPE, start_new_session=True)
+    ck_path = work / "checkpoint.json"
+    try:
+        deadline = time.time() + 60
+        while time.time() < deadline:
+            if ck_path.exists() and json.loads(ck_path.read_text()).get("residues"):
+                break
+            time.sleep(0.1)
+        else:
+            raise AssertionError("no checkpointed residue within 60 s")
+    finally:
+        os.killpg(p.pid, signal.SIGKILL)  # the process group this test started
+        p.communicate(timeout=30)
+    ck = json.loads(ck_path.read_text())
+    assert list(ck["residues"]) == ["4294967291"]
+    r = run(9, work, solver)
+    assert r.returncode == 0 and f"exact={COUNTS[9]}" in r.stdout

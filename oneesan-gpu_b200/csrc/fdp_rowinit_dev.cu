@@ -34,6 +34,10 @@ struct Lanes {
   uint64_t off[16];          // word offset of lane l's panel: L0 * N + (l - L0)
   int pw[16];                // panel width of lane l
   uint32_t c8[16][7];        // 2^(8s) mod p, s = 0..6 (tensor-core product's limb shifts)
+  // Lane groups of the tensor-core product: up to four lanes of one panel,
+  // adjacent in every state's panel words.
+  int ngroups;
+  int grp_lane0[16], grp_n[16];
 };
 
 __device__ __forceinline__ uint32_t red64(unsigned long long x, uint32_t p, unsigned long long m) {
@@ -247,30 +251,52 @@ __global__ void __launch_bounds__(256) rowinit_product_kernel(Lanes ln, int L, i
 // swizzle, core matrices of 8 rows x 16 bytes, 256 bytes between 8-row
 // groups, 128 bytes between the two 16-byte K halves, the four limbs one after
 // the other (128-row A tiles of 16 KB, 64-row B tiles of 8 KB).  The product
-// kernel then streams them with bulk copies into an 8-stage ring: thread 0
-// issues the copies (each stage completes an mbarrier by bytes), the MMAs of a
-// stage as soon as it has landed, and commits them to the stage's "empty"
-// mbarrier, so the copies of the next stages overlap the MMAs.  After an
-// item's last step it commits to an accumulator barrier.  Warps 4..7 then read
-// the seven groups of their rows out of tensor memory into register sums,
-// hand tensor memory back (an mbarrier the issuer waits on before the next
-// item's MMAs), and reduce mod p and store while those MMAs run.  Every wait is bounded.  One
-// CTA per SM (it holds all 512 tensor-memory columns), persistent over
-// (tile, lane) items, lanes innermost so a state's panel words are written
-// close together in time.
+// kernel streams them with bulk copies into a 4-stage ring: thread 0 issues
+// the copies (each stage completes an mbarrier by bytes), the MMAs of a stage
+// as soon as it has landed, and commits them to the stage's "empty" mbarrier,
+// so the copies of the next stages overlap the MMAs.
+//
+// A work item is one 128 x 64 tile for a group of up to four lanes of one
+// panel (the lanes whose words of a state are adjacent in memory).  The lanes
+// of the group are multiplied one after another; after each, warps 4..7 read
+// the seven accumulator groups of their rows out of tensor memory, hand it
+// back (an mbarrier the issuer waits on before the next lane's MMAs), reduce
+// mod p and park the residues in shared memory as [row][column][lane].  Once
+// the group is complete each warp writes its 32 rows: per row 64 consecutive
+// states, every state's group of lanes one 16-, 8- or 4-byte store, so a warp
+// store covers one contiguous run of the panel instead of 32 scattered words.
+// Items run in bands of eight row tiles so that a band's column tiles are
+// read from memory once for all eight.  Every wait is bounded.  One CTA per SM
+// (it holds all 512 tensor-memory columns and 226 KB of shared memory).
 constexpr int MM = 128, MN = 64, MK = 32;
 constexpr int A_LIMB = MM * MK, B_LIMB = MN * MK;         // bytes of one limb's tile per K step
 constexpr int A_TILE = 4 * A_LIMB, B_TILE = 4 * B_LIMB;   // 16 KB, 8 KB
-constexpr int NST = 8;                                    // ring stages
+constexpr int NST = 4;                                    // ring stages
 constexpr uint32_t kIdescI8 = (2u << 4) | (uint32_t(MN >> 3) << 17) | (uint32_t(MM >> 4) << 24);  // S32 += U8 x U8, K-major
+constexpr uint32_t kIdescN256 = (2u << 4) | (uint32_t(4 * MN >> 3) << 17) | (uint32_t(MM >> 4) << 24);
+constexpr uint32_t kIdescN192 = (2u << 4) | (uint32_t(3 * MN >> 3) << 17) | (uint32_t(MM >> 4) << 24);
 constexpr uint32_t kTmemCols = 512;
-constexpr size_t kMmaSmem = NST * (A_TILE + B_TILE);  // the ring: 192 KB, so one CTA per SM
+constexpr int SROW = MN * 4 + 4;                          // staged words per row: 64 states x 4 lanes, padded
+constexpr size_t kRingBytes = size_t(NST) * (A_TILE + B_TILE);
+constexpr size_t kMmaSmem = kRingBytes + size_t(MM) * SROW * 4;  // 96 KB ring + 130 KB staging
+constexpr int RBAND = 8;                                  // row tiles per band of the item order
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
   return uint64_t((saddr >> 4) & 0x3fffu) | (uint64_t(128 >> 4) << 16) | (uint64_t(256 >> 4) << 32) |
          (uint64_t(1) << 46);
+}
+
+// D[tmem] (+)= A x B^T, M = 128, u8 x u8 -> s32; `acc` = 0 overwrites D.
+__device__ __forceinline__ void mma_i8(uint32_t d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred PRED_enable_input_d;\n\t"
+      "setp.ne.b32 PRED_enable_input_d, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, PRED_enable_input_d;\n\t}"
+      :
+      : "r"(d), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+      : "memory");
 }
 
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
@@ -334,14 +360,34 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_
                : "memory");
 }
 
-__global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int L, int K, uint64_t n, uint64_t C,
+// Item it of a product: its row tile, column tile and lane group.  Groups are
+// innermost; row tiles run in bands of RBAND, a band sweeping every column tile.
+__device__ __forceinline__ void mma_item(uint64_t it, int ngroups, uint64_t rblocks, uint64_t cblocks, uint64_t &rb,
+                                         uint64_t &cb, int &grp) {
+  grp = int(it % uint64_t(ngroups));
+  const uint64_t t = it / uint64_t(ngroups);
+  const uint64_t full = rblocks / RBAND, band = uint64_t(RBAND) * cblocks;
+  if (t < full * band) {
+    const uint64_t r = t % band;
+    cb = r / RBAND;
+    rb = (t / band) * RBAND + r % RBAND;
+  } else {
+    const uint64_t tail = rblocks - full * RBAND, r = t - full * band;
+    cb = r / tail;
+    rb = full * RBAND + r % tail;
+  }
+}
+
+__global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int K, uint64_t n, uint64_t C,
                                                              const unsigned char *Ap, const unsigned char *Bp,
                                                              const uint64_t *base, uint32_t *out,
                                                              unsigned int *err) {
-  extern __shared__ __align__(1024) unsigned char dsm[];
+  extern __shared__ __align__(128) unsigned char dsm[];
   __shared__ __align__(8) uint64_t full_bar[NST], empty_bar[NST], acc_full, acc_empty;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
+  volatile int *abort_v = &abort_flag;
+  uint32_t *stage_out = reinterpret_cast<uint32_t *>(dsm + kRingBytes);
   const int t = threadIdx.x, warp = t >> 5;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
@@ -363,149 +409,176 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int L, in
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
   const int nks = (K + MK - 1) / MK;
+  const int ngroups = ln.ngroups;
   const uint64_t rblocks = (n + MM - 1) / MM, cblocks = (C + MN - 1) / MN;
-  const uint64_t items = rblocks * cblocks * uint64_t(L);
+  const uint64_t items = rblocks * cblocks * uint64_t(ngroups);
   const uint64_t my_items = items > blockIdx.x ? (items - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
-  const uint64_t steps = my_items * uint64_t(nks);  // this CTA's K steps, in order
-  // Step g of this CTA: its item, lane, tile and K step.
-  auto decode = [&](uint64_t g, uint64_t &rb, uint64_t &cb, int &l, int &ks) {
-    const uint64_t it = blockIdx.x + (g / uint64_t(nks)) * gridDim.x;
-    ks = int(g % uint64_t(nks));
-    l = int(it % uint64_t(L));
-    const uint64_t tile = it / uint64_t(L);
-    cb = tile % cblocks;
-    rb = tile / cblocks;
-  };
   if (t == 0) {
-    // Producer and MMA issuer: copies run NST - 1 steps ahead of the MMAs;
-    // an item's MMAs start once the epilogue has read the previous item's
-    // accumulators out of tensor memory.
-    uint64_t issued = 0, g = 0;
-    auto issue_copy = [&](uint64_t q) -> bool {
-      const int s = int(q % NST);
-      const uint64_t use = q / NST;
+    // Producer and MMA issuer.  The copy cursor (pk, pl, pks) runs up to
+    // NST - 1 steps ahead of the MMAs; a lane's MMAs start once the epilogue
+    // has read the previous lane's accumulators out of tensor memory.
+    uint64_t pk = 0, prb = 0, pcb = 0;
+    int pl = 0, pks = 0, pgrp = 0;
+    if (my_items) mma_item(blockIdx.x, ngroups, rblocks, cblocks, prb, pcb, pgrp);
+    uint64_t issued = 0, g = 0, lic = 0;
+    auto issue_copy = [&]() -> bool {
+      const int s = int(issued % NST);
+      const uint64_t use = issued / NST;
       if (use > 0 && !mbar_wait(smem_addr(&empty_bar[s]), uint32_t((use - 1) & 1u))) return false;
-      uint64_t rb, cb;
-      int l, ks;
-      decode(q, rb, cb, l, ks);
-      const unsigned char *a = Ap + ((uint64_t(l) * rblocks + rb) * uint64_t(nks) + uint64_t(ks)) * uint64_t(A_TILE);
-      const unsigned char *b = Bp + ((uint64_t(l) * cblocks + cb) * uint64_t(nks) + uint64_t(ks)) * uint64_t(B_TILE);
+      const uint64_t lane = uint64_t(ln.grp_lane0[pgrp] + pl);
+      const unsigned char *a = Ap + ((lane * rblocks + prb) * uint64_t(nks) + uint64_t(pks)) * uint64_t(A_TILE);
+      const unsigned char *b = Bp + ((lane * cblocks + pcb) * uint64_t(nks) + uint64_t(pks)) * uint64_t(B_TILE);
       const uint32_t fb = smem_addr(&full_bar[s]);
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(uint32_t(A_TILE + B_TILE)), "r"(fb)
                    : "memory");
       unsigned char *st = dsm + size_t(s) * (A_TILE + B_TILE);
       bulk_load(smem_addr(st), a, A_TILE, fb);
       bulk_load(smem_addr(st + A_TILE), b, B_TILE, fb);
+      ++issued;
+      if (++pks == nks) {
+        pks = 0;
+        if (++pl == ln.grp_n[pgrp]) {
+          pl = 0;
+          if (++pk < my_items) mma_item(blockIdx.x + pk * gridDim.x, ngroups, rblocks, cblocks, prb, pcb, pgrp);
+        }
+      }
       return true;
     };
-    for (uint64_t item = 0; item < my_items && !abort_flag; ++item) {
-      while (issued < steps && issued < g + NST - 1) {
-        if (!issue_copy(issued)) {
-          abort_flag = 1;
-          break;
+    for (uint64_t k = 0; k < my_items && !*abort_v; ++k) {
+      uint64_t rb, cb;
+      int grp;
+      mma_item(blockIdx.x + k * gridDim.x, ngroups, rblocks, cblocks, rb, cb, grp);
+      for (int li = 0; li < ln.grp_n[grp] && !*abort_v; ++li, ++lic) {
+        while (pk < my_items && issued < g + NST - 1) {
+          if (!issue_copy()) {
+            *abort_v = 1;
+            break;
+          }
         }
-        ++issued;
-      }
-      if (abort_flag) break;
-      if (item > 0 && !mbar_wait(smem_addr(&acc_empty), uint32_t((item - 1) & 1u))) {
-        abort_flag = 1;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      for (int ks = 0; ks < nks; ++ks, ++g) {
-        const int s = int(g % NST);
-        if (!mbar_wait(smem_addr(&full_bar[s]), uint32_t((g / NST) & 1u))) {
-          abort_flag = 1;
+        if (*abort_v) break;
+        if (lic > 0 && !mbar_wait(smem_addr(&acc_empty), uint32_t((lic - 1) & 1u))) {
+          *abort_v = 1;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const unsigned char *st = dsm + size_t(s) * (A_TILE + B_TILE);
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int sft = i + j;
-            const uint32_t en = (ks > 0 || i != (sft > 3 ? sft - 3 : 0)) ? 1u : 0u;
-            const uint64_t da = umma_desc(smem_addr(st + i * A_LIMB)), db = umma_desc(smem_addr(st + A_TILE + j * B_LIMB));
-            asm volatile(
-                "{\n\t.reg .pred PRED_enable_input_d;\n\t"
-                "setp.ne.b32 PRED_enable_input_d, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, PRED_enable_input_d;\n\t}"
-                :
-                : "r"(tmem + uint32_t(sft * MN)), "l"(da), "l"(db), "r"(kIdescI8), "r"(en)
-                : "memory");
-          }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_addr(&empty_bar[s]))
-                     : "memory");
-        // Refill the stage of step g - 1 (its MMAs were issued before these
-        // ones) with step g + NST - 1 while this step's MMAs run.
-        if (issued < steps && issued == g + NST - 1) {
-          if (!issue_copy(issued)) {
-            abort_flag = 1;
+        for (int ks = 0; ks < nks; ++ks, ++g) {
+          const int s = int(g % NST);
+          if (!mbar_wait(smem_addr(&full_bar[s]), uint32_t((g / NST) & 1u))) {
+            *abort_v = 1;
             break;
           }
-          ++issued;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const unsigned char *st = dsm + size_t(s) * (A_TILE + B_TILE);
+          // The B tile's four limbs are one 256-row operand, so A limb i times
+          // all of B is one N = 256 MMA whose column block j lands at
+          // 64 (i + j), the accumulator of its shift.  The first step writes
+          // each accumulator fresh once: limb 0 covers shifts 0..3, and limb
+          // i >= 1 adds onto shifts i..i+2 and starts shift i + 3.
+          const uint64_t dA = umma_desc(smem_addr(st)), dB = umma_desc(smem_addr(st + A_TILE));
+          if (ks > 0) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) mma_i8(tmem + uint32_t(i * MN), dA + uint64_t(i * (A_LIMB >> 4)), dB, kIdescN256, 1u);
+          } else {
+            mma_i8(tmem, dA, dB, kIdescN256, 0u);
+#pragma unroll
+            for (int i = 1; i < 4; ++i) {
+              const uint64_t da = dA + uint64_t(i * (A_LIMB >> 4));
+              mma_i8(tmem + uint32_t(i * MN), da, dB, kIdescN192, 1u);
+              mma_i8(tmem + uint32_t((i + 3) * MN), da, dB + uint64_t(3 * (B_LIMB >> 4)), kIdescI8, 0u);
+            }
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           smem_addr(&empty_bar[s]))
+                       : "memory");
+          // Refill the stage of step g - 1 (its MMAs were issued before these
+          // ones) with step g + NST - 1 while this step's MMAs run.
+          if (pk < my_items && issued == g + NST - 1 && !issue_copy()) {
+            *abort_v = 1;
+            break;
+          }
         }
+        if (*abort_v) break;
+        // The lane's accumulators are complete once its MMAs are.
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&acc_full))
+                     : "memory");
       }
-      // The item's accumulators are complete once its MMAs are.
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_addr(&acc_full))
-                   : "memory");
     }
   } else if (warp >= 4) {
-    // Epilogue warps 4..7: warp w reads tensor-memory lanes 32 (w - 4) .. + 31
-    // (the tile's rows), sums the limb groups of its row's 64 outputs into
-    // registers, hands tensor memory back, then reduces and stores while the
-    // next item's MMAs run.  G_s < 4 K 255^2 < 2^28 (K <= 1024), so
-    // sum_s G_s (2^(8s) mod p) < 7 x 2^60 fits 64 bits.
-    const int quarter = warp - 4;
-    for (uint64_t item = 0; item < my_items; ++item) {
-      if (!mbar_wait(smem_addr(&acc_full), uint32_t(item & 1u))) {
-        abort_flag = 1;
-        break;
-      }
-      if (abort_flag) break;
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // Epilogue warps 4..7: warp w owns tensor-memory lanes (tile rows)
+    // 32 (w - 4) .. + 31 and the same rows of the staging buffer, so only
+    // the warp itself reads back what it parked there.  G_s < 4 K 255^2 <
+    // 2^28 (K <= 1024), so sum_s G_s (2^(8s) mod p) < 7 x 2^60 fits 64 bits.
+    const int quarter = warp - 4, lane_t = t & 31, row = quarter * 32 + lane_t;
+    uint32_t *my_row = stage_out + size_t(row) * SROW;
+    uint64_t lic = 0;
+    for (uint64_t k = 0; k < my_items && !*abort_v; ++k) {
       uint64_t rb, cb;
-      int l, ks0;
-      decode(item * uint64_t(nks), rb, cb, l, ks0);
-      unsigned long long acc[MN];
-#pragma unroll
-      for (int q = 0; q < MN; ++q) acc[q] = 0;
-#pragma unroll
-      for (int c = 0; c < MN; c += 16) {
-#pragma unroll
-        for (int sft = 0; sft < 7; ++sft) {
-          uint32_t gv[16];
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-              "%14, %15}, [%16];"
-              : "=r"(gv[0]), "=r"(gv[1]), "=r"(gv[2]), "=r"(gv[3]), "=r"(gv[4]), "=r"(gv[5]), "=r"(gv[6]),
-                "=r"(gv[7]), "=r"(gv[8]), "=r"(gv[9]), "=r"(gv[10]), "=r"(gv[11]), "=r"(gv[12]), "=r"(gv[13]),
-                "=r"(gv[14]), "=r"(gv[15])
-              : "r"(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(sft * MN + c)));
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          const uint32_t cs = ln.c8[l][sft];
-#pragma unroll
-          for (int q = 0; q < 16; ++q) acc[c + q] += (unsigned long long)gv[q] * cs;
+      int grp;
+      mma_item(blockIdx.x + k * gridDim.x, ngroups, rblocks, cblocks, rb, cb, grp);
+      const int G = ln.grp_n[grp], lane0 = ln.grp_lane0[grp];
+      const uint64_t gi_mine = rb * MM + uint64_t(row), j0 = cb * MN;
+      const uint64_t my_base = gi_mine < n ? base[gi_mine] : 0;
+      bool ok = true;
+      for (int li = 0; li < G; ++li, ++lic) {
+        if (!mbar_wait(smem_addr(&acc_full), uint32_t(lic & 1u))) {
+          *abort_v = 1;
+          ok = false;
+          break;
         }
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&acc_empty)) : "memory");
-      const uint64_t gi = rb * MM + uint64_t(quarter * 32 + (t & 31)), j0 = cb * MN;
-      if (gi < n) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int l = lane0 + li;
+        unsigned long long acc[MN];
+#pragma unroll
+        for (int q = 0; q < MN; ++q) acc[q] = 0;
+#pragma unroll
+        for (int c = 0; c < MN; c += 16) {
+#pragma unroll
+          for (int sft = 0; sft < 7; ++sft) {
+            uint32_t gv[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15}, [%16];"
+                : "=r"(gv[0]), "=r"(gv[1]), "=r"(gv[2]), "=r"(gv[3]), "=r"(gv[4]), "=r"(gv[5]), "=r"(gv[6]),
+                  "=r"(gv[7]), "=r"(gv[8]), "=r"(gv[9]), "=r"(gv[10]), "=r"(gv[11]), "=r"(gv[12]), "=r"(gv[13]),
+                  "=r"(gv[14]), "=r"(gv[15])
+                : "r"(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(sft * MN + c)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const uint32_t cs = ln.c8[l][sft];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) acc[c + q] += (unsigned long long)gv[q] * cs;
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&acc_empty)) : "memory");
         const uint32_t p = ln.p[l];
         const unsigned long long m = ln.m[l];
-        const uint64_t b0 = base[gi];
-        uint32_t *o = out + ln.off[l];
-        const uint64_t pw = uint64_t(ln.pw[l]);
 #pragma unroll
-        for (int q = 0; q < MN; ++q) {
-          const uint64_t gj = j0 + uint64_t(q);
-          if (gj < C) o[(b0 + gj) * pw] = red64(acc[q], p, m);
+        for (int q = 0; q < MN; ++q) my_row[q * 4 + li] = red64(acc[q], p, m);
+      }
+      if (!ok) break;
+      __syncwarp();
+      // Write the warp's 32 rows: row r holds states base[r] + j0 .. + 63,
+      // each state's G lanes adjacent in the panel (G words from the group's
+      // first lane, 4 G-byte aligned: panels start at multiples of their width).
+      const uint32_t pw = uint32_t(ln.pw[lane0]);
+      uint32_t *o = out + ln.off[lane0];
+      for (int rr = 0; rr < 32; ++rr) {
+        const uint64_t b0 = __shfl_sync(0xffffffffu, my_base, rr);
+        if (rb * MM + uint64_t(quarter * 32 + rr) >= n) break;  // the same for the whole warp
+        const uint32_t *src = stage_out + size_t(quarter * 32 + rr) * SROW;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int q = lane_t + 32 * h;
+          if (j0 + uint64_t(q) >= C) continue;
+          const uint4 v = *reinterpret_cast<const uint4 *>(src + q * 4);
+          uint32_t *dst = o + (b0 + j0 + uint64_t(q)) * pw;
+          if (G == 4) *reinterpret_cast<uint4 *>(dst) = v;
+          else if (G == 2) *reinterpret_cast<uint2 *>(dst) = make_uint2(v.x, v.y);
+          else *dst = v.x;
         }
       }
+      __syncwarp();
     }
   }
   __syncthreads();
@@ -718,6 +791,11 @@ cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mo
       ln.off[l + i] = uint64_t(l) * pl.states + uint64_t(i);
       ln.pw[l + i] = pw;
     }
+    for (int g0 = 0; g0 < pw; g0 += 4) {
+      ln.grp_lane0[ln.ngroups] = l + g0;
+      ln.grp_n[ln.ngroups] = std::min(4, pw - g0);
+      ++ln.ngroups;
+    }
     l += pw;
   }
   for (int l = 0; l < L; ++l) {
@@ -792,9 +870,9 @@ cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mo
       rowinit_pack_kernel<<<pblocks, 256, 0, s>>>(U + prevU.base[h], cols, K, L, MN, bp);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       n += 2;
-      const uint64_t items = rblocks * cblocks * uint64_t(L);
+      const uint64_t items = rblocks * cblocks * uint64_t(ln.ngroups);
       const uint64_t grid = std::min<uint64_t>(items, uint64_t(device_sm_count()));
-      rowinit_mma_kernel<<<unsigned(grid), 256, kMmaSmem, s>>>(ln, L, K, rows_h, cols, ap, bp,
+      rowinit_mma_kernel<<<unsigned(grid), 256, kMmaSmem, s>>>(ln, K, rows_h, cols, ap, bp,
                                                                 d->base_hr + d->base_hoff[size_t(h)], main, d->err);
     } else {
       const uint64_t tiles = ((rows_h + TM - 1) / TM) * ((cols + TN - 1) / TN);

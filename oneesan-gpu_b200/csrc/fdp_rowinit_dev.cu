@@ -4,11 +4,13 @@
 //                   edges into q' of v_parent[q] x weight (mod p per lane);
 //   suffix levels : one warp per completion, u[q] = sum over the edges out of
 //                   q of weight x u_child[q'];
-//   products      : per end height h, out[base_x + j] = v_x . U_h[j] as a
-//                   tiled product of 64 prefixes x 64 completions.  The
-//                   suffix values are split into 16-bit halves so that every
-//                   partial sum of 32 x 16-bit products stays below 2^64 for
-//                   up to 2^16 terms; one Barrett reduction per output.
+//   products      : per end height h, out[base_x + j] = v_x . U_h[j], on the
+//                   tensor cores (rowinit_mma_kernel: u8 limbs, s32
+//                   accumulators in tensor memory, K <= 1024) or on the CUDA
+//                   cores (rowinit_product_kernel: 64 prefixes x 64
+//                   completions per tile, suffix values split into 16-bit
+//                   halves so that every partial sum stays below 2^64 for up
+//                   to 2^16 terms); one Barrett reduction per output either way.
 // Scratch (two prefix levels, two suffix levels) is the caller's; the state
 // vector is written in the lane-panel layout of the cell kernels.
 #include <algorithm>

@@ -81,6 +81,15 @@ typedef struct fdp_plan_out {
   uint64_t alg_bytes_per_residue;   /* sum over cells of fdp_cell_bytes            */
   uint64_t transitions_per_residue; /* sum over cells of (M + D)                  */
   int fits;                         /* total_bytes <= budget                      */
+  uint64_t sweep_peak_bytes;        /* device bytes held during the row sweeps:
+                                       state, every width table of the pass
+                                       (bounded spaces included), small buffers
+                                       (the PLAN line's dp_peak_gib)            */
+  uint64_t init_peak_bytes;         /* device bytes held while the row-k
+                                       initialiser fills the state: the above
+                                       plus its tables; its scratch is the
+                                       blocked state (the PLAN line's
+                                       row6_peak_gib)                           */
 } fdp_plan_out;
 
 /* Per-call timing (the reference reports wall_s and phase sums, GB.cu:2257). */
@@ -317,13 +326,24 @@ fdp_status fdp_reverse2_apply(fdp_ctx *ctx, int width, int p, int lanes, const u
  * `moduli` is host memory.  The dot product's 64-bit accumulators live in a
  * fixed array inside the library (128 bytes, 16 lanes), so widths above 28
  * or more than 16 lanes are rejected with FDP_ERR_ARGS.  The first call on a
- * device, with that device current, looks the array up and copies a count
- * table in; make that first call before any stream capture.  Every call on a
- * device shares the array; each call clears it on `stream` first, but calls
- * that overlap on the GPU race on it and must be serialised.
+ * device, with that device current, looks the array's device address up and
+ * keeps it; make that first call before any stream capture, and do not call
+ * this entry point again after destroying the device's primary context
+ * (cudaDeviceReset).  Every call on a device shares the array; each call
+ * clears it on `stream` first, but calls that overlap on the GPU race on it
+ * and must be serialised.
  */
 fdp_status fdp_first_row_dot_noalloc(int width, int lanes, const uint32_t *moduli, const uint32_t *d_main,
                                      uint32_t *d_residues, void *stream);
+
+/*
+ * Fault injection for tests: the next `count` computations (a run_sync or
+ * run_multi_sync problem, a served request) start with their device error
+ * word already set, exactly as when one of their kernels gives up on a bounded
+ * wait, so that each entry point's failure report can be checked without
+ * making a kernel fail.  No counterpart in the reference.
+ */
+fdp_status fdp_test_inject_pass_errors(int count);
 
 /* Canonical rank / unrank of frontier words on the device (GB.cu:1568 rank_full). */
 fdp_status fdp_rank_words(fdp_ctx *ctx, int width, const uint64_t *d_words, uint64_t *d_ranks, uint64_t count,

@@ -1,4 +1,5 @@
 // C ABI of the frontier-DP engine (include/oneesan_fdp.h).
+#include <atomic>
 #include <chrono>
 #include <map>
 #include <mutex>
@@ -99,6 +100,12 @@ extern "C" fdp_status fdp_plan(const fdp_problem *pr, uint64_t budget, fdp_plan_
     o.alg_bytes_per_residue += fdp::row_bytes(W, cap);
     o.transitions_per_residue += uint64_t(o.cells_per_row) * fdp::cell_transitions(W, cap);
   }
+  // Width tables a pass uploads: the full space, each bounded space and the
+  // height-1 space of row 0; the expansion tables fit in the 1 MiB margin.
+  const uint64_t ntables = 1 + (caps.empty() ? 0 : caps.size() + 1);
+  o.sweep_peak_bytes = o.state_bytes + ntables * o.table_bytes + (1u << 20);
+  o.init_peak_bytes = o.sweep_peak_bytes + (R >= 2 ? fdp::row_init_tables(W, R, rcap) : 0);
+  o.total_bytes = o.init_peak_bytes > o.sweep_peak_bytes ? o.init_peak_bytes : o.sweep_peak_bytes;
   o.fits = o.total_bytes <= budget ? 1 : 0;
   *out = o;
   return FDP_OK;
@@ -124,6 +131,8 @@ extern "C" fdp_status fdp_create(fdp_ctx **out, int device) {
   if (s == FDP_OK) s = cuda_status(cudaMalloc(&c->d_acc, sizeof(unsigned long long) * FDP_MAX_LANES), "acc");
   if (s == FDP_OK) s = cuda_status(cudaMalloc(&c->d_res, sizeof(uint32_t) * FDP_MAX_LANES), "res");
   if (s == FDP_OK) s = cuda_status(cudaMallocHost(&c->h_res, sizeof(uint32_t) * FDP_RUN_MAX_MODULI), "pinned res");
+  if (s == FDP_OK) s = cuda_status(cudaMalloc(&c->d_err, sizeof(unsigned int)), "error word");
+  if (s == FDP_OK) s = cuda_status(cudaMallocHost(&c->h_err, sizeof(unsigned int)), "pinned error word");
   if (s == FDP_OK) s = cuda_status(cudaEventCreate(&c->ev0), "event");
   if (s == FDP_OK) s = cuda_status(cudaEventCreate(&c->ev1), "event");
   if (s != FDP_OK) {
@@ -144,6 +153,8 @@ fdp_ctx::~fdp_ctx() {
   if (d_acc) cudaFree(d_acc);
   if (d_res) cudaFree(d_res);
   if (h_res) cudaFreeHost(h_res);
+  if (d_err) cudaFree(d_err);
+  if (h_err) cudaFreeHost(h_err);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (stream) cudaStreamDestroy(stream);
@@ -226,9 +237,30 @@ static fdp_status ensure_buffer(uint32_t **buf, size_t *cap, size_t bytes, const
 // space is small; the state grows in place between them (the blocked buffer,
 // dead at row boundaries, stages the move).  `blk` must hold D x L words of
 // the full space.
+// Test hook: the next `count` error-word resets write a nonzero value, as if
+// a kernel had given up on a bounded wait (fdp_test_inject_pass_errors).
+static std::atomic<int> g_injected_errors{0};
+
+cudaError_t fdp_enqueue_err_reset(unsigned int *d_err, cudaStream_t s) {
+  int v = g_injected_errors.load();
+  while (v > 0 && !g_injected_errors.compare_exchange_weak(v, v - 1)) {
+  }
+  return cudaMemsetAsync(d_err, v > 0 ? 1 : 0, sizeof(unsigned int), s);
+}
+
+cudaError_t fdp_enqueue_err_read(unsigned int *h_err, const unsigned int *d_err, cudaStream_t s) {
+  return cudaMemcpyAsync(h_err, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
+}
+
+extern "C" fdp_status fdp_test_inject_pass_errors(int count) {
+  if (count < 0) return FDP_ERR_ARGS;
+  g_injected_errors.store(count);
+  return FDP_OK;
+}
+
 fdp_status fdp_enqueue_pass(fdp_ctx *c, const DevTables &t, int L, const uint32_t *mods, uint32_t *main,
                             uint32_t *blk, unsigned long long *acc, uint32_t *d_res, uint32_t *h_res,
-                            cudaStream_t s, uint64_t *launches) {
+                            unsigned int *d_err, cudaStream_t s, uint64_t *launches) {
   const int W = t.W;
   const uint64_t M = fdp::main_states(W), D = fdp::blocked_states(W);
   uint64_t n = 0;
@@ -251,7 +283,8 @@ fdp_status fdp_enqueue_pass(fdp_ctx *c, const DevTables &t, int L, const uint32_
     // Rows 0..R-1 at once: the state after row R-1, filled into row R's space
     // (the blocked buffer is the fill's scratch).
     if ((st = space(rcap, &prev)) != FDP_OK) return st;
-    FDP_CK(fdp::enqueue_row_init(W, R, rcap, L, mods, main, blk, D * uint64_t(L), c->cfg.row_init_tensor, s, &n),
+    FDP_CK(fdp::enqueue_row_init(W, R, rcap, L, mods, main, blk, D * uint64_t(L), c->cfg.row_init_tensor, d_err, s,
+                                 &n),
            "row-k initialiser");
     next_row = R;
   } else if (B > 0) {
@@ -313,12 +346,13 @@ extern "C" fdp_status fdp_run_sync(fdp_ctx *c, const fdp_problem *pr, uint32_t *
   cudaGraphExec_t ge = nullptr;
   FDP_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
   uint64_t launches = 0;
-  fdp_status es = FDP_OK;
+  fdp_status es = cuda_status(fdp_enqueue_err_reset(c->d_err, c->stream), "error word");
   for (int done = 0; done < pr->k && es == FDP_OK; done += lanes) {
     const int L = (pr->k - done) < lanes ? (pr->k - done) : lanes;
     es = fdp_enqueue_pass(c, *t, L, pr->moduli + done, c->d_main, c->d_blk, c->d_acc, c->d_res, c->h_res + done,
-                          c->stream, &launches);
+                          c->d_err, c->stream, &launches);
   }
+  if (es == FDP_OK) es = cuda_status(fdp_enqueue_err_read(c->h_err, c->d_err, c->stream), "error word");
   cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
   if (es != FDP_OK) {
     if (g) cudaGraphDestroy(g);
@@ -336,13 +370,9 @@ extern "C" fdp_status fdp_run_sync(fdp_ctx *c, const fdp_problem *pr, uint32_t *
   cudaGraphExecDestroy(ge);
   FDP_CK(ce, "graph launch");
   FDP_CK(se, "residue pass");
-  {
-    int rcap = 0;
-    const int R = row_init_rows(c, W, &rcap);
-    if (R && c->cfg.row_init_tensor && fdp::row_init_failed(W, R, rcap)) {
-      g_last_error = "row-k initialiser: a bounded wait of the tensor-core product gave up";
-      return FDP_ERR_CUDA;
-    }
+  if (*c->h_err) {
+    g_last_error = "residue pass: a bounded wait on the device gave up; the residues are invalid";
+    return FDP_ERR_CUDA;
   }
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -498,6 +528,7 @@ struct MultiPart {
   int lanes = 1;
   uint32_t *main = nullptr, *blk = nullptr, *res = nullptr;
   unsigned long long *acc = nullptr;
+  unsigned int *err = nullptr;  // this problem's error word
   cudaStream_t s = nullptr;
   cudaEvent_t done = nullptr;
 };
@@ -530,6 +561,7 @@ extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, i
       if (p.blk) cudaFree(p.blk);
       if (p.acc) cudaFree(p.acc);
       if (p.res) cudaFree(p.res);
+      if (p.err) cudaFree(p.err);
       if (p.s) cudaStreamDestroy(p.s);
       if (p.done) cudaEventDestroy(p.done);
     }
@@ -541,7 +573,8 @@ extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, i
     rs = cuda_status((expr), (what));          \
     if (rs != FDP_OK) { cleanup(); return rs; } \
   } while (0)
-  MULTI_CK(cudaMallocHost(&pinned, sizeof(uint32_t) * size_t(total_k)), "pinned residues");
+  // Residues of every problem, then one error word per problem.
+  MULTI_CK(cudaMallocHost(&pinned, sizeof(uint32_t) * size_t(total_k + count)), "pinned residues");
   MULTI_CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
   for (int i = 0; i < count; ++i) {
     MultiPart &p = parts[size_t(i)];
@@ -552,6 +585,7 @@ extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, i
     MULTI_CK(cudaMalloc(&p.blk, size_t(fdp::blocked_states(W)) * p.lanes * 4 + 4), "multi blocked state");
     MULTI_CK(cudaMalloc(&p.acc, sizeof(unsigned long long) * FDP_MAX_LANES), "multi acc");
     MULTI_CK(cudaMalloc(&p.res, sizeof(uint32_t) * FDP_MAX_LANES), "multi res");
+    MULTI_CK(cudaMalloc(&p.err, sizeof(unsigned int)), "multi error word");
     MULTI_CK(cudaStreamCreateWithFlags(&p.s, cudaStreamNonBlocking), "multi stream");
     MULTI_CK(cudaEventCreateWithFlags(&p.done, cudaEventDisableTiming), "multi event");
   }
@@ -562,11 +596,15 @@ extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, i
   for (int i = 0; i < count && rs == FDP_OK; ++i) {
     MultiPart &p = parts[size_t(i)];
     cudaStreamWaitEvent(p.s, fork, 0);
+    rs = cuda_status(fdp_enqueue_err_reset(p.err, p.s), "error word");
     for (int done = 0; done < probs[i].k && rs == FDP_OK; done += p.lanes) {
       const int L = (probs[i].k - done) < p.lanes ? (probs[i].k - done) : p.lanes;
       rs = fdp_enqueue_pass(c, *p.t, L, probs[i].moduli + done, p.main, p.blk, p.acc, p.res, pinned + off + done,
-                            p.s, &launches);
+                            p.err, p.s, &launches);
     }
+    if (rs == FDP_OK)
+      rs = cuda_status(fdp_enqueue_err_read(reinterpret_cast<unsigned int *>(pinned + total_k + i), p.err, p.s),
+                       "error word");
     cudaEventRecord(p.done, p.s);
     cudaStreamWaitEvent(c->stream, p.done, 0);
     off += probs[i].k;
@@ -582,6 +620,13 @@ extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, i
   MULTI_CK(cudaStreamSynchronize(c->stream), "multi pass");
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  for (int i = 0; i < count; ++i)
+    if (pinned[total_k + i]) {
+      g_last_error = "multi pass: a bounded wait on the device gave up in problem " + std::to_string(i) +
+                     "; the residues are invalid";
+      cleanup();
+      return FDP_ERR_CUDA;
+    }
   for (int i = 0; i < total_k; ++i) residues_out[i] = pinned[i];
   if (st) {
     fdp_run_stats acc{};

@@ -18,6 +18,8 @@ struct fdp_ctx {
   unsigned long long *d_acc = nullptr;   // first-row dot accumulators
   uint32_t *d_res = nullptr;             // residues on the device
   uint32_t *h_res = nullptr;             // residues, pinned host
+  unsigned int *d_err = nullptr;         // run_sync pass error word (device)
+  unsigned int *h_err = nullptr;         // its copy after the pass (pinned host)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   fdp::LaunchCfg cfg;
   std::mutex mu;         // serialises run_sync / apply_cells / time_cells / tuning
@@ -31,7 +33,14 @@ fdp_status fdp_ctx_tables_cap(fdp_ctx *c, int W, int cap, const fdp::DevTables *
 fdp_status fdp_prepare_pass(fdp_ctx *c, int W, const fdp::DevTables **full);
 fdp_status fdp_enqueue_pass(fdp_ctx *c, const fdp::DevTables &t, int L, const uint32_t *mods, uint32_t *main,
                             uint32_t *blk, unsigned long long *acc, uint32_t *d_res, uint32_t *h_res,
-                            cudaStream_t s, uint64_t *launches);
+                            unsigned int *d_err, cudaStream_t s, uint64_t *launches);
+// A computation's error word: a kernel that gives up on a bounded wait writes
+// a nonzero value to it.  Each computation (a run_sync graph, one problem of a
+// run_multi_sync graph, one served request) owns its word in its own buffers;
+// the reset is enqueued before its passes and the read-back after them, on the
+// same stream, so concurrent computations never see each other's failures.
+cudaError_t fdp_enqueue_err_reset(unsigned int *d_err, cudaStream_t s);
+cudaError_t fdp_enqueue_err_read(unsigned int *h_err, const unsigned int *d_err, cudaStream_t s);
 void fdp_set_last_error(const char *msg);
 fdp_status fdp_cuda_status(cudaError_t e, const char *what);
 void fdp_server_shutdown(fdp_ctx *c);

@@ -1,6 +1,8 @@
 // Explicit instantiations of the cell / first-row kernels for K in
 // [FDP_K_LO, FDP_K_HI]; the build compiles this file once per K range so the
 // 2 x 16 kernel variants build in parallel.
+#include <mutex>
+
 #include "fdp_kernels.cuh"
 #include "fdp_launch.h"
 
@@ -13,28 +15,51 @@
 
 namespace fdp {
 
+// Per-device launch state of one kernel variant: the dynamic shared-memory
+// limit is raised once per device to the largest record store of the largest
+// CTA, and the occupancy of every (CTA size, record size) is resolved on first
+// use on that device.
+constexpr int kInstMaxDevices = 64;
+constexpr int kBlockSizes = 256 / 32;  // CTA sizes 32 .. 256 in steps of 32
+
+struct VariantState {
+  bool limit_set = false;
+  int per_sm[kBlockSizes + 1][FDP_REC_MAX_ITEMS + 1] = {};  // 0: not resolved yet
+};
+
 template <typename Idx, int K>
 cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t s) {
+  static std::mutex mu;
+  static VariantState state[kInstMaxDevices];
+  if (cfg.block < 32 || cfg.block > 256 || cfg.block % 32) return cudaErrorInvalidValue;
   const int rec_items = a.compact ? a.lane_items : 0;  // <= FDP_REC_MAX_ITEMS (launch_cell)
   const size_t smem = cell_smem_bytes<Idx, K>(cfg.block, rec_items);
-  // Per-variant state, resolved on first use (the device is the same for the
-  // life of the process in this library's contexts): the shared-memory limit
-  // is raised to the largest record store once, and occupancy is known for
-  // every record size.
-  static int configured_block = 0, per_sm[FDP_REC_MAX_ITEMS + 1] = {};
-  if (configured_block != cfg.block) {
-    const size_t most = cell_smem_bytes<Idx, K>(cfg.block, FDP_REC_MAX_ITEMS);
-    cudaError_t e = cudaFuncSetAttribute(cell_kernel<Idx, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(most));
-    if (e != cudaSuccess) return e;
-    for (int c = 0; c <= FDP_REC_MAX_ITEMS; ++c) {
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[c], cell_kernel<Idx, K>, cfg.block,
-                                                        cell_smem_bytes<Idx, K>(cfg.block, c));
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kInstMaxDevices) return cudaErrorInvalidDevice;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    VariantState &v = state[dev];
+    if (!v.limit_set) {
+      const size_t most = cell_smem_bytes<Idx, K>(256, FDP_REC_MAX_ITEMS);
+      e = cudaFuncSetAttribute(cell_kernel<Idx, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(most));
       if (e != cudaSuccess) return e;
-      if (per_sm[c] < 1) per_sm[c] = 1;
+      v.limit_set = true;
     }
-    configured_block = cfg.block;
+    int &slot = v.per_sm[cfg.block / 32][rec_items];
+    if (slot == 0) {
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&slot, cell_kernel<Idx, K>, cfg.block, smem);
+      if (e != cudaSuccess) {
+        slot = 0;
+        return e;
+      }
+      if (slot < 1) slot = 1;
+    }
+    per_sm = slot;
   }
-  int grid = cfg.grid > 0 ? cfg.grid : device_sm_count() * per_sm[rec_items];
+  int grid = cfg.grid > 0 ? cfg.grid : device_sm_count() * per_sm;
   const uint64_t per_block = uint64_t(cfg.block) * uint64_t(a.lane_items < 1 ? 1 : a.lane_items);
   const uint64_t need = (a.items + per_block - 1) / per_block;
   if (uint64_t(grid) > need) grid = int(need ? need : 1);

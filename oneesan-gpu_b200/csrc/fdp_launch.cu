@@ -345,22 +345,27 @@ __global__ void ternary_index_kernel(const uint32_t *codes, uint32_t *index, uin
   }
 }
 
+// The count table of the rank / unrank kernels, uploaded once per device.
 static RankTable *rank_table() {
-  static RankTable *d = nullptr;
-  static int dev_of = -1;
+  static std::mutex mu;
+  static std::map<int, RankTable *> per_dev;
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (d && dev_of == dev) return d;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = per_dev.find(dev);
+  if (it != per_dev.end()) return it->second;
   RankTable h;
   const CountTable &c = counts();
   for (int w = 0; w <= FDP_MAXW; ++w)
     for (int k = 0; k < FDP_HT; ++k) h.H[w][k] = c.H[w][k];
   RankTable *p = nullptr;
   if (cudaMalloc(&p, sizeof(h)) != cudaSuccess) return nullptr;
-  if (cudaMemcpy(p, &h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
-  d = p;
-  dev_of = dev;
-  return d;
+  if (cudaMemcpy(p, &h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(p);
+    return nullptr;
+  }
+  per_dev[dev] = p;
+  return p;
 }
 
 static unsigned grid_for(uint64_t count) {

@@ -15,10 +15,14 @@
 // buffer the library allocates.  Limits: width <= 28 and lanes <= 16.
 //
 // Set-up: the first call on a device (with that device current) looks up the
-// device address of the arrays with cudaGetSymbolAddress and copies the count
-// table in with cudaMemcpyToSymbol; do that first call before any stream
-// capture.  Host code must never pass the array names themselves to a kernel:
-// in host code they are host-side stand-ins, not device addresses.
+// device address of the array with cudaGetSymbolAddress and keeps it for the
+// life of the process; do that first call before any stream capture.  The
+// address belongs to the device's primary context: a caller that destroys it
+// (cudaDeviceReset) must not call this entry point again in the same process.
+// Host code must never pass the array's name itself to a kernel: in host code
+// it is a host-side stand-in, not a device address.  The kernel builds the
+// canonical-rank count table in its own shared memory, so nothing else is
+// uploaded.
 //
 // Every call on a device shares the same accumulators and they keep the last
 // call's contents; each call clears them on its stream before use.  Calls
@@ -41,13 +45,10 @@ using ull = unsigned long long;
 
 // Scratch: the dot product's per-lane 64-bit accumulators (128 bytes).
 static __device__ __align__(256) ull g_noalloc_acc[FDP_NOALLOC_MAX_LANES];
-// Read-only: H[w][h] counts for the canonical rank (7.9 KB).
-static __device__ __align__(256) ull g_noalloc_counts[(FDP_MAXW + 1) * FDP_HT];
 
 struct DeviceSetup {
   bool ready = false;
-  ull *acc = nullptr;     // device address of g_noalloc_acc
-  ull *counts = nullptr;  // device address of g_noalloc_counts
+  ull *acc = nullptr;  // device address of g_noalloc_acc
 };
 std::mutex g_setup_mu;
 DeviceSetup g_setup[FDP_NOALLOC_MAX_DEVICES];
@@ -57,12 +58,20 @@ struct Mods {
 };
 
 template <int K>
-__global__ void __launch_bounds__(256) noalloc_dot_kernel(const ull *__restrict__ counts, const uint32_t *main,
-                                                          uint64_t mstates, ull *acc_out, int W) {
+__global__ void __launch_bounds__(256) noalloc_dot_kernel(const uint32_t *main, uint64_t mstates, ull *acc_out,
+                                                          int W) {
   __shared__ ull sH[FDP_MAXW + 1][FDP_HT];
   __shared__ ull red[8][K];
-  for (int i = threadIdx.x; i < (FDP_MAXW + 1) * FDP_HT; i += blockDim.x) (&sH[0][0])[i] = counts[i];
+  // H[w][h]: words of w symbols from height h down to 0 (N keeps the height,
+  // R lowers it, L raises it), built row by row: the canonical-rank counts.
+  if (threadIdx.x < FDP_HT) sH[0][threadIdx.x] = threadIdx.x == 0 ? 1ull : 0ull;
   __syncthreads();
+  for (int w = 1; w <= FDP_MAXW; ++w) {
+    const int h = int(threadIdx.x);
+    if (h < FDP_HT)
+      sH[w][h] = sH[w - 1][h] + (h > 0 ? sH[w - 1][h - 1] : 0ull) + (h + 1 < FDP_HT ? sH[w - 1][h + 1] : 0ull);
+    __syncthreads();
+  }
   const uint64_t total = 1ull << (W - 1);
   ull acc[K];
 #pragma unroll
@@ -99,7 +108,7 @@ cudaError_t launch_dot(const DeviceSetup &s, const uint32_t *main, int W, cudaSt
   const uint64_t total = 1ull << (W - 1);
   uint64_t blocks = (total + 255) / 256;
   if (blocks > 1184) blocks = 1184;
-  noalloc_dot_kernel<K><<<unsigned(blocks), 256, 0, st>>>(s.counts, main, fdp::main_states(W), s.acc, W);
+  noalloc_dot_kernel<K><<<unsigned(blocks), 256, 0, st>>>(main, fdp::main_states(W), s.acc, W);
   return cudaGetLastError();
 }
 
@@ -131,22 +140,14 @@ fdp_status fail(cudaError_t e, const char *what) {
   return FDP_ERR_CUDA;
 }
 
-// Once per device, with that device current: resolve the arrays' device
-// addresses and fill the count table.
+// Once per device, with that device current: resolve the array's device
+// address.
 fdp_status setup_device(int dev, DeviceSetup **out) {
   std::lock_guard<std::mutex> lk(g_setup_mu);
   DeviceSetup &s = g_setup[dev];
   if (!s.ready) {
     cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&s.acc), g_noalloc_acc);
     if (e != cudaSuccess) return fail(e, "cudaGetSymbolAddress(accumulators)");
-    e = cudaGetSymbolAddress(reinterpret_cast<void **>(&s.counts), g_noalloc_counts);
-    if (e != cudaSuccess) return fail(e, "cudaGetSymbolAddress(counts)");
-    static ull host_counts[(FDP_MAXW + 1) * FDP_HT];
-    const fdp::CountTable &c = fdp::counts();
-    for (int w = 0; w <= FDP_MAXW; ++w)
-      for (int h = 0; h < FDP_HT; ++h) host_counts[w * FDP_HT + h] = c.H[w][h];
-    e = cudaMemcpyToSymbol(g_noalloc_counts, host_counts, sizeof(host_counts));
-    if (e != cudaSuccess) return fail(e, "cudaMemcpyToSymbol(counts)");
     s.ready = true;
   }
   *out = &s;

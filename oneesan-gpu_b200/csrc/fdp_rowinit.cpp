@@ -387,6 +387,28 @@ RowInitPlan plan_row_init(int W, int rows, int cap) {
   return pl;
 }
 
+uint64_t row_init_table_bytes(const RowInitPlan &pl) {
+  const RowAutomaton &a = row_automaton(pl.rows);
+  uint64_t b = 0;
+  // Automaton: state ids, first-column edges (3 + 1 offsets, targets and
+  // weights), interior edges both ways (3 x (states + 1) offsets each, one
+  // index and one weight per edge), last-column weights (3 x states).
+  uint64_t inner = 0, first = 0;
+  for (int s = 0; s < 3; ++s) {
+    inner += a.inner[s].size();
+    first += a.first[s].size();
+  }
+  b += 4 * uint64_t(a.nstates) + 4 * 4 + 8 * first + 2 * (12 * uint64_t(a.nstates + 1) + 8 * inner) +
+       12 * uint64_t(a.nstates);
+  // Prefix trie: parent and row (4 bytes each), symbol and height (1 byte
+  // each) per prefix of every level, and the last level's state bases.
+  uint64_t prefixes = 0;
+  for (int k = 0; k < pl.P; ++k) prefixes += pl.parent[size_t(k)].size();
+  b += 10 * prefixes;
+  if (pl.P > 0) b += 8 * pl.parent[size_t(pl.P - 1)].size();
+  return b;
+}
+
 uint64_t row_init_scratch_words(const RowInitPlan &pl) {
   uint64_t pre = 0, suf = 0;
   for (int k = 0; k < pl.P; ++k) {

@@ -87,6 +87,10 @@ RowInitPlan plan_row_init(int W, int rows, int cap);
 // suffix levels (the larger of each pair of consecutive levels).
 uint64_t row_init_scratch_words(const RowInitPlan &plan);
 
+// Device bytes of the fill's tables (automaton and prefix trie) for a plan;
+// they stay resident once uploaded for that (W, rows, cap).
+uint64_t row_init_table_bytes(const RowInitPlan &plan);
+
 // The fill computed on the host for one modulus (reference for the device
 // kernels and their tests): the whole target-space vector.
 std::vector<uint32_t> row_init_fill_host(const RowInitPlan &plan, uint32_t mod);

@@ -301,7 +301,12 @@ __device__ __forceinline__ void mma_i8(uint32_t d, uint64_t da, uint64_t db, uin
       : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+// Bounded wait for the completion of phase `phase` of an mbarrier: false after
+// 2^22 polls, or (with `abort` given) as soon as another thread of the CTA
+// has raised the abort flag, so that one give-up ends every role's waits
+// quickly.  A wait that gives up leaves its asynchronous operation in flight;
+// rowinit_mma_kernel drains those before it frees tensor memory and exits.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, const volatile int *abort = nullptr) {
   for (int i = 0; i < (1 << 22); ++i) {
     uint32_t done;
     asm volatile(
@@ -312,6 +317,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
         : "r"(bar), "r"(phase)
         : "memory");
     if (done) return true;
+    if (abort && (i & 255) == 255 && *abort) return false;
   }
   return false;
 }
@@ -385,7 +391,7 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int K, ui
                                                              const uint64_t *base, uint32_t *out,
                                                              unsigned int *err) {
   extern __shared__ __align__(128) unsigned char dsm[];
-  __shared__ __align__(8) uint64_t full_bar[NST], empty_bar[NST], acc_full, acc_empty;
+  __shared__ __align__(8) uint64_t full_bar[NST], empty_bar[NST], acc_full, acc_empty, drain_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   volatile int *abort_v = &abort_flag;
@@ -404,6 +410,7 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int K, ui
     }
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&acc_full)), "r"(1) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&acc_empty)), "r"(128) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&drain_bar)), "r"(1) : "memory");
     abort_flag = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -426,7 +433,7 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int K, ui
     auto issue_copy = [&]() -> bool {
       const int s = int(issued % NST);
       const uint64_t use = issued / NST;
-      if (use > 0 && !mbar_wait(smem_addr(&empty_bar[s]), uint32_t((use - 1) & 1u))) return false;
+      if (use > 0 && !mbar_wait(smem_addr(&empty_bar[s]), uint32_t((use - 1) & 1u), abort_v)) return false;
       const uint64_t lane = uint64_t(ln.grp_lane0[pgrp] + pl);
       const unsigned char *a = Ap + ((lane * rblocks + prb) * uint64_t(nks) + uint64_t(pks)) * uint64_t(A_TILE);
       const unsigned char *b = Bp + ((lane * cblocks + pcb) * uint64_t(nks) + uint64_t(pks)) * uint64_t(B_TILE);
@@ -458,14 +465,14 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int K, ui
           }
         }
         if (*abort_v) break;
-        if (lic > 0 && !mbar_wait(smem_addr(&acc_empty), uint32_t((lic - 1) & 1u))) {
+        if (lic > 0 && !mbar_wait(smem_addr(&acc_empty), uint32_t((lic - 1) & 1u), abort_v)) {
           *abort_v = 1;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         for (int ks = 0; ks < nks; ++ks, ++g) {
           const int s = int(g % NST);
-          if (!mbar_wait(smem_addr(&full_bar[s]), uint32_t((g / NST) & 1u))) {
+          if (!mbar_wait(smem_addr(&full_bar[s]), uint32_t((g / NST) & 1u), abort_v)) {
             *abort_v = 1;
             break;
           }
@@ -506,6 +513,19 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int K, ui
                      : "memory");
       }
     }
+    if (*abort_v) {
+      // Drain before the CTA frees tensor memory and its shared memory: a
+      // commit to drain_bar arrives once every MMA this thread issued has
+      // completed, and each bulk copy issued but never consumed (steps
+      // g .. issued-1, one per ring stage at most) completes its stage's
+      // full barrier.  Both waits are bounded; a drain that still gives up
+      // leaves the error flag set all the same.
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_addr(&drain_bar))
+                   : "memory");
+      mbar_wait(smem_addr(&drain_bar), 0u);
+      for (uint64_t c = g; c < issued; ++c) mbar_wait(smem_addr(&full_bar[c % NST]), uint32_t((c / NST) & 1u));
+    }
   } else if (warp >= 4) {
     // Epilogue warps 4..7: warp w owns tensor-memory lanes (tile rows)
     // 32 (w - 4) .. + 31 and the same rows of the staging buffer, so only
@@ -523,7 +543,7 @@ __global__ void __launch_bounds__(256, 1) rowinit_mma_kernel(Lanes ln, int K, ui
       const uint64_t my_base = gi_mine < n ? base[gi_mine] : 0;
       bool ok = true;
       for (int li = 0; li < G; ++li, ++lic) {
-        if (!mbar_wait(smem_addr(&acc_full), uint32_t(lic & 1u))) {
+        if (!mbar_wait(smem_addr(&acc_full), uint32_t(lic & 1u), abort_v)) {
           *abort_v = 1;
           ok = false;
           break;
@@ -598,7 +618,6 @@ struct RowInitDevice {
   uint8_t *sym = nullptr, *height = nullptr;
   uint64_t *base_hr = nullptr;  // level P bases by (height, row)
   std::vector<uint64_t> base_hoff;
-  unsigned int *err = nullptr;  // set by the tensor-core product if a bounded wait gave up
   ~RowInitDevice() {
     for (void *p : allocs) cudaFree(p);
   }
@@ -704,8 +723,6 @@ cudaError_t build_device(int W, int rows, int cap, std::unique_ptr<RowInitDevice
   for (size_t i = 0; i < htop.size(); ++i) bhr[size_t(d->base_hoff[htop[i]]) + size_t(rtop[i])] = pl.base[i];
   UP(bhr, d->base_hr)
 #undef UP
-  std::vector<unsigned int> zero(1, 0u);
-  if ((e = upload(*d, zero, &d->err)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(rowinit_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMmaSmem))) !=
       cudaSuccess)
     return e;
@@ -744,35 +761,28 @@ cudaError_t prepare_row_init(int W, int rows, int cap) {
 
 int auto_row_init_rows(int W) { return W >= 18 ? 7 : (W >= 14 ? 6 : 0); }
 
-bool row_init_failed(int W, int rows, int cap) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return false;
-  unsigned int *flag = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    auto it = g_cache.find(std::make_tuple(dev, W, rows, cap));
-    if (it == g_cache.end()) return false;
-    flag = it->second->err;
-  }
-  unsigned int h = 0;
-  if (cudaMemcpy(&h, flag, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
-  if (h) cudaMemset(flag, 0, sizeof(h));
-  return h != 0;
-}
-
-uint64_t row_init_scratch(int W, int rows, int cap) {
+// Scratch words per lane and table bytes of a fill plan, computed once per
+// (W, rows, cap): planning large widths takes a moment on the host.
+static std::pair<uint64_t, uint64_t> row_init_sizes(int W, int rows, int cap) {
   static std::mutex mu;
-  static std::map<std::tuple<int, int, int>, uint64_t> words;
+  static std::map<std::tuple<int, int, int>, std::pair<uint64_t, uint64_t>> sizes;
   std::lock_guard<std::mutex> lk(mu);
   auto key = std::make_tuple(W, rows, cap);
-  auto it = words.find(key);
-  if (it == words.end()) it = words.emplace(key, row_init_scratch_words(plan_row_init(W, rows, cap))).first;
+  auto it = sizes.find(key);
+  if (it == sizes.end()) {
+    const RowInitPlan pl = plan_row_init(W, rows, cap);
+    it = sizes.emplace(key, std::make_pair(row_init_scratch_words(pl), row_init_table_bytes(pl))).first;
+  }
   return it->second;
 }
 
+uint64_t row_init_scratch(int W, int rows, int cap) { return row_init_sizes(W, rows, cap).first; }
+
+uint64_t row_init_tables(int W, int rows, int cap) { return row_init_sizes(W, rows, cap).second; }
+
 cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mods, uint32_t *main,
-                             uint32_t *scratch, uint64_t scratch_words, bool tensor, cudaStream_t s,
-                             uint64_t *launches) {
+                             uint32_t *scratch, uint64_t scratch_words, bool tensor, unsigned int *err,
+                             cudaStream_t s, uint64_t *launches) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -784,7 +794,7 @@ cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mo
     d = it->second.get();
   }
   const RowInitPlan &pl = d->plan;
-  if (L < 1 || L > 16) return cudaErrorInvalidValue;
+  if (L < 1 || L > 16 || (tensor && !err)) return cudaErrorInvalidValue;
   if (row_init_scratch_words(pl) * uint64_t(L) > scratch_words) return cudaErrorInvalidValue;
   Lanes ln{};
   for (int l = 0; l < L;) {
@@ -875,7 +885,7 @@ cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mo
       const uint64_t items = rblocks * cblocks * uint64_t(ln.ngroups);
       const uint64_t grid = std::min<uint64_t>(items, uint64_t(device_sm_count()));
       rowinit_mma_kernel<<<unsigned(grid), 256, kMmaSmem, s>>>(ln, K, rows_h, cols, ap, bp,
-                                                                d->base_hr + d->base_hoff[size_t(h)], main, d->err);
+                                                                d->base_hr + d->base_hoff[size_t(h)], main, err);
     } else {
       const uint64_t tiles = ((rows_h + TM - 1) / TM) * ((cols + TN - 1) / TN);
       rowinit_product_kernel<<<unsigned(tiles), 256, 0, s>>>(ln, L, K, rows_h, cols, V + prevA.base[h],

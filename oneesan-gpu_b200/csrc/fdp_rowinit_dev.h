@@ -18,16 +18,17 @@ int auto_row_init_rows(int W);
 // Scratch words per lane the fill needs (two prefix and two suffix levels).
 uint64_t row_init_scratch(int W, int rows, int cap);
 
+// Device bytes of the fill's resident tables (automaton, prefix trie).
+uint64_t row_init_tables(int W, int rows, int cap);
+
 // Enqueue the fill of `main` (L lanes, panel layout, the target space's
 // states) on `s`, using `scratch` (scratch_words words, not overlapping main).
 // tensor: the products on the tensor cores (tcgen05, 8-bit limbs) instead of
-// the CUDA cores.
+// the CUDA cores; a tensor-core product whose bounded wait gives up writes a
+// nonzero value to the caller's device word `err` (required when tensor), and
+// its residues are then invalid.
 cudaError_t enqueue_row_init(int W, int rows, int cap, int L, const uint32_t *mods, uint32_t *main,
-                             uint32_t *scratch, uint64_t scratch_words, bool tensor, cudaStream_t s,
-                             uint64_t *launches);
-
-// Whether a tensor-core product gave up on a bounded wait since the last call
-// (and clear the flag); host-synchronous.
-bool row_init_failed(int W, int rows, int cap);
+                             uint32_t *scratch, uint64_t scratch_words, bool tensor, unsigned int *err,
+                             cudaStream_t s, uint64_t *launches);
 
 }  // namespace fdp

@@ -83,7 +83,9 @@ struct Job {
   int n = 0, lanes = 1, passes = 1, slot = -1;
   std::vector<uint32_t> mods, residues;
   uint64_t bytes = 0, off = 0;
-  enum State { QUEUED, RUNNING, DONE, FAILED } state = QUEUED;
+  // LAUNCHING: admitted (slot and pool range reserved), being captured and
+  // launched by the scheduler with the lock released.
+  enum State { QUEUED, LAUNCHING, RUNNING, DONE, FAILED } state = QUEUED;
   fdp_status status = FDP_OK;
   std::string error;
   Clock::time_point t_submit, t_admit, t_done;
@@ -92,7 +94,8 @@ struct Job {
 };
 
 // Bytes of one request in the pool: the state for `lanes` residues, then the
-// dot-product accumulators and device residues.
+// dot-product accumulators (256 bytes), and the device residues with the
+// request's error word 128 bytes after them (256 bytes).
 uint64_t request_bytes(int n, int lanes) {
   const int W = n + 1;
   const uint64_t M = fdp::main_states(W), D = fdp::blocked_states(W);
@@ -110,7 +113,7 @@ struct fdp_server {
   PoolAlloc alloc;
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> ev_start, ev_done;
-  std::vector<uint32_t *> pinned;  // per slot, kMaxModuliPerRequest residues
+  std::vector<uint32_t *> pinned;  // per slot, kMaxModuliPerRequest residues, then the error word
   std::vector<Job *> slot_job;
   std::deque<uint64_t> queue;
   std::map<uint64_t, std::unique_ptr<Job>> jobs;
@@ -144,16 +147,19 @@ struct fdp_server {
     char *small = base + j->bytes - 2 * kAlign;
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(small);
     uint32_t *dres = reinterpret_cast<uint32_t *>(small + kAlign);
+    unsigned int *derr = reinterpret_cast<unsigned int *>(small + kAlign + 128);
+    unsigned int *herr = reinterpret_cast<unsigned int *>(pinned[size_t(slot)] + kMaxModuliPerRequest);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return fdp_cuda_status(e, "serve: begin capture");
-    fdp_status es = FDP_OK;
+    fdp_status es = fdp_cuda_status(fdp_enqueue_err_reset(derr, s), "serve: error word");
     uint64_t launches = 0;
     for (int done = 0; done < int(j->mods.size()) && es == FDP_OK; done += j->lanes) {
       const int L = std::min(j->lanes, int(j->mods.size()) - done);
-      es = fdp_enqueue_pass(ctx, *t, L, j->mods.data() + done, main, blk, acc, dres, pinned[size_t(slot)] + done, s,
-                            &launches);
+      es = fdp_enqueue_pass(ctx, *t, L, j->mods.data() + done, main, blk, acc, dres, pinned[size_t(slot)] + done,
+                            derr, s, &launches);
     }
+    if (es == FDP_OK) es = fdp_cuda_status(fdp_enqueue_err_read(herr, derr, s), "serve: error word");
     e = cudaStreamEndCapture(s, &g);
     if (es != FDP_OK) {
       if (g) cudaGraphDestroy(g);
@@ -179,7 +185,10 @@ struct fdp_server {
     if (j->exec) cudaGraphExecDestroy(j->exec);
     j->exec = nullptr;
     j->t_done = Clock::now();
-    if (ok) {
+    const unsigned int herr = pinned[size_t(slot)][kMaxModuliPerRequest];
+    if (ok && herr) {
+      fail(j, FDP_ERR_CUDA, "serve: a bounded wait on the device gave up; the residues are invalid");
+    } else if (ok) {
       float ms = 0;
       cudaEventElapsedTime(&ms, ev_start[size_t(slot)], ev_done[size_t(slot)]);
       j->device_s = ms * 1e-3;
@@ -207,37 +216,50 @@ struct fdp_server {
         queue.clear();
         if (!running) break;
       }
-      // (2) admission, arrival order with bounded backfill
-      const Clock::time_point now = Clock::now();
-      for (auto it = queue.begin(); it != queue.end() && running < cfg.max_active;) {
-        Job *j = jobs[*it].get();
+      // (2) admission, arrival order with bounded backfill.  A request is
+      // taken off the queue with its slot and pool range reserved under the
+      // lock; its tables, capture, instantiation and launch then run with the
+      // lock released, so fdp_submit / fdp_poll / fdp_wait never wait for
+      // them.  Only this thread changes slots and the pool.
+      while (running < cfg.max_active) {
+        const Clock::time_point now = Clock::now();
+        Job *j = nullptr;
         int slot = -1;
         for (int s = 0; s < int(slot_job.size()); ++s)
           if (!slot_job[size_t(s)]) { slot = s; break; }
-        uint64_t off = 0;
-        if (slot >= 0 && alloc.alloc(j->bytes, &off)) {
-          j->off = off;
-          j->slot = slot;
-          j->t_admit = now;
-          slot_job[size_t(slot)] = j;
-          ++running;
-          peak_running = std::max(peak_running, running);
-          it = queue.erase(it);
-          fdp_status st = launch(j);
-          if (st != FDP_OK) {
-            slot_job[size_t(slot)] = nullptr;
-            --running;
-            alloc.release(j->off, j->bytes);
-            if (j->exec) cudaGraphExecDestroy(j->exec);
-            j->exec = nullptr;
-            fail(j, st, std::string("serve: launch failed: ") + fdp_last_error());
-          } else {
-            j->state = Job::RUNNING;
+        if (slot < 0) break;
+        for (auto it = queue.begin(); it != queue.end(); ++it) {
+          Job *q = jobs[*it].get();
+          uint64_t off = 0;
+          if (alloc.alloc(q->bytes, &off)) {
+            q->off = off;
+            j = q;
+            queue.erase(it);
+            break;
           }
-          continue;
+          if (it == queue.begin() && secs(q->t_submit, now) > cfg.max_bypass_s) break;  // reserve for the head
         }
-        if (it == queue.begin() && secs(j->t_submit, now) > cfg.max_bypass_s) break;  // reserve for the head
-        ++it;
+        if (!j) break;
+        j->slot = slot;
+        j->t_admit = now;
+        j->state = Job::LAUNCHING;
+        slot_job[size_t(slot)] = j;
+        ++running;
+        peak_running = std::max(peak_running, running);
+        lk.unlock();
+        const fdp_status st = launch(j);
+        const std::string why = st != FDP_OK ? std::string(fdp_last_error()) : std::string();
+        lk.lock();
+        if (st != FDP_OK) {
+          slot_job[size_t(slot)] = nullptr;
+          --running;
+          alloc.release(j->off, j->bytes);
+          if (j->exec) cudaGraphExecDestroy(j->exec);
+          j->exec = nullptr;
+          fail(j, st, "serve: launch failed: " + why);
+        } else {
+          j->state = Job::RUNNING;
+        }
       }
       cv.notify_all();  // wake fdp_wait callers
       if (!running && queue.empty() && !stopping) cv.wait(lk);
@@ -283,7 +305,8 @@ extern "C" fdp_status fdp_server_start(fdp_ctx *c, const fdp_server_config *cfg)
     if (st == FDP_OK) st = fdp_cuda_status(cudaEventCreate(&sv->ev_start[i]), "server event");
     if (st == FDP_OK) st = fdp_cuda_status(cudaEventCreate(&sv->ev_done[i]), "server event");
     if (st == FDP_OK)
-      st = fdp_cuda_status(cudaMallocHost(&sv->pinned[i], sizeof(uint32_t) * kMaxModuliPerRequest), "server pinned");
+      st = fdp_cuda_status(cudaMallocHost(&sv->pinned[i], sizeof(uint32_t) * (kMaxModuliPerRequest + 1)),
+                           "server pinned");
   }
   if (st != FDP_OK) {
     for (size_t i = 0; i < S; ++i) {
@@ -374,7 +397,7 @@ static fdp_status take_result(fdp_server *sv, uint64_t id, uint32_t *out, fdp_re
   auto it = sv->jobs.find(id);
   if (it == sv->jobs.end()) return FDP_ERR_NOT_FOUND;
   Job *j = it->second.get();
-  if (j->state == Job::QUEUED || j->state == Job::RUNNING) return FDP_PENDING;
+  if (j->state == Job::QUEUED || j->state == Job::LAUNCHING || j->state == Job::RUNNING) return FDP_PENDING;
   if (info) {
     info->queue_s = j->slot >= 0 || j->state == Job::DONE ? secs(j->t_submit, j->t_admit) : secs(j->t_submit, j->t_done);
     info->run_s = j->state == Job::DONE ? secs(j->t_admit, j->t_done) : 0.0;

@@ -73,17 +73,25 @@ int main(int argc, char **argv) {
     return exit_code(s);
   }
   if (const char *e = getenv("GRIDFP_PLAN_ONLY"); e && atoi(e) != 0) {
+    // One `PLAN n=` line of key=value tokens, the memory plan the reference's
+    // autotuner reads (scripts/run/autotune.py:189-200): it requires exactly
+    // one such line with n= and gpus= equal to its request, and admits a
+    // configuration when scratch_fits=1 and max(dp_peak_gib, row6_peak_gib)
+    // plus its reserve fits every device's free memory.  This engine runs on
+    // one GPU: a request for more is planned as not fitting.
+    const int gpus = requested > 0 ? requested : 1;
+    const double gib = double(1ull << 30);
     fprintf(stderr,
-            "PLAN n=%d W=%d gpus=1 main=%llu blocked=%llu auth_gib=%.6f lanes=%d passes=%d index_bits=%d init_rows=%d "
-            "state_gib=%.6f scratch_gib=0 table_mib=%.3f total_gib=%.6f rows=%d cells_per_row=%d "
-            "alg_bytes_per_residue=%llu transitions_per_residue=%llu scratch_limit_mib=%d max_window=%d "
-            "scratch_fits=1\n",
-            n, plan.width, (unsigned long long)plan.main_states, (unsigned long long)plan.blocked_states,
-            double(plan.main_states + plan.blocked_states) * 4.0 / double(1ull << 30), plan.lanes, plan.passes,
-            plan.index_bits, plan.init_rows, double(plan.state_bytes) / double(1ull << 30), double(plan.table_bytes) / (1 << 20),
-            double(plan.total_bytes) / double(1ull << 30), plan.rows, plan.cells_per_row,
-            (unsigned long long)plan.alg_bytes_per_residue, (unsigned long long)plan.transitions_per_residue,
-            target_mib, max_window);
+            "PLAN n=%d W=%d gpus=%d main=%llu blocked=%llu auth_gib=%.6f lanes=%d passes=%d index_bits=%d "
+            "init_rows=%d state_gib=%.6f scratch_gib=0 table_mib=%.3f total_gib=%.6f dp_peak_gib=%.6f "
+            "row6_peak_gib=%.6f rows=%d cells_per_row=%d alg_bytes_per_residue=%llu transitions_per_residue=%llu "
+            "scratch_limit_mib=%d max_window=%d scratch_fits=%d\n",
+            n, plan.width, gpus, (unsigned long long)plan.main_states, (unsigned long long)plan.blocked_states,
+            double(plan.main_states + plan.blocked_states) * 4.0 / gib, plan.lanes, plan.passes, plan.index_bits,
+            plan.init_rows, double(plan.state_bytes) / gib, double(plan.table_bytes) / (1 << 20),
+            double(plan.total_bytes) / gib, double(plan.sweep_peak_bytes) / gib, double(plan.init_peak_bytes) / gib,
+            plan.rows, plan.cells_per_row, (unsigned long long)plan.alg_bytes_per_residue,
+            (unsigned long long)plan.transitions_per_residue, target_mib, max_window, gpus == 1 ? 1 : 0);
     fprintf(stderr, "PLAN crt_moduli=%zu", mods.size());
     for (uint32_t m : mods) fprintf(stderr, " %u:ok", m);
     fprintf(stderr, "\n");

@@ -48,7 +48,8 @@ class PlanOut(ctypes.Structure):
                 ("rows", ctypes.c_int), ("bounded_rows", ctypes.c_int), ("init_rows", ctypes.c_int),
                 ("cells_per_row", ctypes.c_int),
                 ("alg_bytes_per_residue", ctypes.c_uint64),
-                ("transitions_per_residue", ctypes.c_uint64), ("fits", ctypes.c_int)]
+                ("transitions_per_residue", ctypes.c_uint64), ("fits", ctypes.c_int),
+                ("sweep_peak_bytes", ctypes.c_uint64), ("init_peak_bytes", ctypes.c_uint64)]
 
 
 class Tuning(ctypes.Structure):
@@ -136,6 +137,7 @@ def lib() -> ctypes.CDLL:
         getattr(L, name).restype = c_u64
     L.fdp_cell_bytes.argtypes = [c_int, c_int]
     L.fdp_cell_bytes.restype = c_u64
+    L.fdp_test_inject_pass_errors.argtypes = [c_int]
     _lib = L
     return L
 
@@ -191,6 +193,12 @@ def blocked_states(width: int) -> int:
 
 def cell_bytes(width: int, p: int) -> int:
     return int(lib().fdp_cell_bytes(width, p))
+
+
+def inject_pass_errors(count: int) -> None:
+    """Test hook: the next `count` computations start with their device error
+    word set, as when a kernel gives up on a bounded wait."""
+    _check(lib().fdp_test_inject_pass_errors(count), "fdp_test_inject_pass_errors")
 
 
 def plan(n: int, moduli: Sequence[int], lanes: int | None = None, budget: int = 1 << 62) -> PlanOut:

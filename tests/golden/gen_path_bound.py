@@ -2,13 +2,15 @@
 """Regenerate tests/golden/path_bound.json from the reference's own
 scripts/solve/path_bound.py (needs the reference tree; run from the repo root):
 
-    python tests/golden/gen_path_bound.py /root/reference
+    python tests/golden/gen_path_bound.py <reference tree>
 """
 import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2 or not os.path.isfile(os.path.join(sys.argv[1], "scripts", "solve", "path_bound.py")):
+    sys.exit("usage: gen_path_bound.py <reference tree containing scripts/solve/path_bound.py>")
+ref = sys.argv[1]
 sys.path.insert(0, os.path.join(ref, "scripts", "solve"))
 import path_bound  # noqa: E402
 

@@ -13,6 +13,18 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
 GGCOUNT = os.path.join(ROOT, "oracle", "_ref", "ggcount_multi")
+REFERENCE_ROOT_FILE = os.path.join(ROOT, "oracle", "_ref", "reference_root")
+
+
+def reference_root():
+    """The reference tree, for CPU tests that import its own Python tools:
+    ONEESAN_REFERENCE_ROOT if set, else the tree `make -C oracle ref
+    REF_ROOT=...` built oracle/_ref from; None when neither is present."""
+    root = os.environ.get("ONEESAN_REFERENCE_ROOT")
+    if not root and os.path.exists(REFERENCE_ROOT_FILE):
+        with open(REFERENCE_ROOT_FILE) as f:
+            root = f.read().strip()
+    return root if root and os.path.isdir(root) else None
 
 # The first 48 primes below 2^32 in descending order: the reference's CRT prime
 # table (scripts/solve/path_bound.py:5-18) is exactly this sequence.

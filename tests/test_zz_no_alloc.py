@@ -59,6 +59,57 @@ def test_noalloc_matches_run_sync_on_two_calls(engine):
         assert got == want
 
 
+def _final_state(engine, n, moduli, stream=0):
+    """The final state of an n residue pass, in caller-owned torch buffers,
+    built through fdp_apply_cells on `stream` (a cudaStream_t, 0: the engine's)."""
+    import torch
+    W, lanes = n + 1, len(moduli)
+    M, D = fdp.main_states(W), fdp.blocked_states(W)
+    init = np.zeros((M, lanes), dtype=np.uint32)
+    for mask in range(1 << (W - 1)):
+        init[orc.rank(int(orc.lib().oracle_first_row_state(mask, W)), W), :] = 1
+    dm = torch.from_numpy(fdp.pack_lanes(init).view(np.int32)).cuda()
+    db = torch.zeros(D * lanes, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    for _row in range(1, W - 1):
+        engine.apply_cells(W, W - 1, 1, moduli, dm.data_ptr(), db.data_ptr(), stream)
+    torch.cuda.synchronize()
+    return dm
+
+
+@pytest.mark.parametrize("lanes", [1, 4, 8, 14, 16])
+def test_noalloc_every_panel_layout(engine, lanes):
+    # 1, 4 and 8 lanes are one panel; 14 is panels {0-7}, {8-11}, {12-13}; 16 is
+    # the fixed scratch's limit, two 8-wide panels.
+    import torch
+    n = 9
+    moduli = orc.largest_primes_below_2_32(lanes)
+    dm = _final_state(engine, n, moduli)
+    want = engine.residues(n, moduli, lanes=lanes).residues
+    for _call in range(2):
+        out = torch.full((lanes,), -1, dtype=torch.int32, device="cuda")
+        assert noalloc(n + 1, moduli, dm.data_ptr(), out.data_ptr()) == fdp.FDP_OK
+        torch.cuda.synchronize()
+        assert [int(x) for x in out.cpu().numpy().view(np.uint32)] == want
+
+
+def test_noalloc_on_a_caller_stream(engine):
+    # The caller's own (non-default) stream orders the state, the read-out and
+    # the copy back; two calls in a row on it.
+    import torch
+    n, lanes = 10, 14
+    moduli = orc.largest_primes_below_2_32(lanes)
+    s = torch.cuda.Stream()
+    dm = _final_state(engine, n, moduli, stream=s.cuda_stream)
+    want = engine.residues(n, moduli, lanes=lanes).residues
+    for _call in range(2):
+        with torch.cuda.stream(s):
+            out = torch.full((lanes,), -1, dtype=torch.int32, device="cuda")
+        assert noalloc(n + 1, moduli, dm.data_ptr(), out.data_ptr(), s.cuda_stream) == fdp.FDP_OK
+        s.synchronize()
+        assert [int(x) for x in out.cpu().numpy().view(np.uint32)] == want
+
+
 def test_noalloc_rejects_sizes_beyond_its_fixed_scratch():
     import torch
     dummy = torch.zeros(64, dtype=torch.int32, device="cuda")

@@ -16,8 +16,12 @@ roofline the per-cell transition kernel: algorithmic bytes per launch
          change, per modulus) over its CUDA-event duration.
 
 --impl reference times the reference's own CPU counter (third_party/ggcount,
-built unmodified into oracle/_ref) on a bounded sample and scales it to the
-same workload by frontier transitions.
+built unmodified into oracle/_ref) on all host threads: each step is one
+n = 18 residue (the plain configuration the reference's CPU path runs), scaled
+to residues/hour at n = 22 by the ratio of frontier transitions per residue
+(stated in the line).  Measured here, that ratio favours the CPU counter: its
+n = 20 residue takes 12.4x its n = 18 residue, where transitions grow 9.8x.
+That arm loads nothing of this repository's engine.
 
 Multi-GPU: replicas only (moduli are independent; no data-path collective).
 Each rank runs the same workload; value is the sum over ranks.
@@ -165,48 +169,95 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+CPU_SAMPLE_N = 18          # the plain configuration the reference's CPU path runs
+CPU_SAMPLE_MOD = 4294967291
+CPU_SAMPLE_RESIDUE = 503411004  # docs/results/reverse-algorithm-2026-09-05.md:53 of the reference
+
+
 def ggcount_sample(threads: int | None = None):
-    """Time the reference's CPU counter on one bounded sample: n=17, one modulus."""
+    """Time the reference's CPU counter on one residue: n = 18 mod 4294967291,
+    all host threads (OpenMP)."""
     import oracle_lib as orc
     exe = orc.GGCOUNT
-    n_s, mod = 17, 4294967291
-    if not os.path.exists(exe):
-        try:
-            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
-                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
-        except (OSError, subprocess.CalledProcessError):
-            pass
+    n_s, mod = CPU_SAMPLE_N, CPU_SAMPLE_MOD
     env = dict(os.environ)
     cores = threads or os.cpu_count() or 1
     env["OMP_NUM_THREADS"] = str(cores)
-    t0 = time.perf_counter()
     if os.path.exists(exe):
+        t0 = time.perf_counter()
         out = subprocess.run([exe, "-q", str(n_s), f"%{mod}"], check=True, capture_output=True, text=True,
                              env=env).stdout
+        dt = time.perf_counter() - t0
         kind = "reference"
         res = int(out.split()[0])
-    else:  # reference tree absent and nothing prebuilt: the oracle port, 1 thread
+        if res != CPU_SAMPLE_RESIDUE:
+            raise SystemExit(f"ggcount n={n_s} mod {mod} gave {res}, expected {CPU_SAMPLE_RESIDUE}")
+    else:  # nothing prebuilt: the oracle port, one thread, a smaller grid
         n_s = 13
+        t0 = time.perf_counter()
         res = orc.residue(n_s, mod)
+        dt = time.perf_counter() - t0
         kind, cores = "port", 1
-    dt = time.perf_counter() - t0
-    return {"n": n_s, "modulus": mod, "residue": res, "seconds": dt, "kind": kind, "cores": cores}
+    return {"n": n_s, "modulus": mod, "residue": res, "seconds": dt, "kind": kind, "cores": cores,
+            "cpu": cpu_model(), "nproc": os.cpu_count()}
 
 
 def transitions_per_residue(n: int) -> int:
-    import fdp
+    """Frontier transitions of a full residue (every row swept): (W-2) rows x
+    (W-1) cells x (M + D) states, with M, D the canonical state counts (words
+    of W and W-1 symbols from height 1 to 0, N keeps the height, R lowers and
+    L raises it).  Pure Python: the reference arm loads none of the engine."""
     W = n + 1
-    return (W - 2) * (W - 1) * (fdp.main_states(W) + fdp.blocked_states(W))
+    H = [[0] * (W + 3) for _ in range(W + 1)]
+    H[0][0] = 1
+    for w in range(1, W + 1):
+        for h in range(W + 2):
+            H[w][h] = H[w - 1][h] + (H[w - 1][h - 1] if h else 0) + H[w - 1][h + 1]
+    return (W - 2) * (W - 1) * (H[W][1] + H[W - 1][1])
+
+
+def cpu_scale(sample: dict, n: int) -> float:
+    """Factor from the sample's seconds per residue to size n's, by frontier
+    transitions per residue."""
+    return transitions_per_residue(n) / transitions_per_residue(sample["n"])
 
 
 def scale_cpu(sample: dict, n: int) -> float:
     """CPU residues/hour at size n, scaled from the sample by frontier transitions."""
-    rate = transitions_per_residue(sample["n"]) / sample["seconds"]
-    return 3600.0 * rate / transitions_per_residue(n)
+    return 3600.0 / (sample["seconds"] * cpu_scale(sample, n))
+
+
+def cpu_baseline_record(sample: dict, n: int, value: float) -> dict:
+    return {"value": value, "unit": "residues/hour", "cores": sample["cores"], "kind": sample["kind"],
+            "cpu": sample["cpu"], "nproc": sample["nproc"],
+            "sample": (f"ggcount_multi -q {sample['n']} %{sample['modulus']}: one residue "
+                       f"({sample['residue']}) in {sample['seconds']:.2f} s on {sample['cores']} threads, "
+                       f"scaled to n={n} by frontier transitions per residue (x{cpu_scale(sample, n):.2f})"),
+            "scale_to_n": n, "scale_factor": cpu_scale(sample, n), "sample_seconds": sample["seconds"]}
+
+
+def bench_config(n: int, k: int, world: int) -> dict:
+    """The workload, the same object in both arms' lines."""
+    return {"workload": f"n={n} exact count: the {k} largest primes below 2^32 (the CRT primes the "
+                        f"checkerboard-strip bound needs)", "n": n, "moduli": k,
+            "l2": "state far larger than L2 (126 MB); no flush needed",
+            "parallelism": f"replicas x{world}"}
 
 
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     vals, samples = [], []
@@ -215,21 +266,18 @@ def run_reference(args) -> None:
         if i >= args.warmup:
             vals.append(scale_cpu(s, args.n))
             samples.append(s)
-    v = sum(vals) / len(vals)
-    s0 = samples[-1]
-    sample_txt = (f"ggcount_multi -q {s0['n']} %{s0['modulus']} (one residue, {s0['cores']} threads, "
-                  f"{s0['seconds']:.2f} s), scaled to n={args.n} by frontier transitions per residue")
+    mean_s = statistics.mean(x["seconds"] for x in samples)
+    s0 = dict(samples[-1], seconds=mean_s)
+    v = scale_cpu(s0, args.n)
     line = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "residues/hour", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000 * statistics.mean(x["seconds"] for x in samples),
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "residues/hour", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * mean_s,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-        "data": "none: the DP state is generated by the initialiser",
-        "config": {"workload": f"n={args.n} exact count, {args.k} largest primes below 2^32", "n": args.n,
-                   "moduli": args.k},
-        "cpu_baseline": {"value": v, "unit": "residues/hour", "cores": s0["cores"], "kind": s0["kind"],
-                         "sample": sample_txt},
+        "data": "none: the DP has no input data",
+        "config": bench_config(args.n, args.k, world),
+        "cpu_baseline": cpu_baseline_record(s0, args.n, v),
         "e2e": {"value": v, "unit": "residues/hour", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "step_seconds": [x["seconds"] for x in samples],
     }
     print(json.dumps(line), flush=True)
 
@@ -344,20 +392,21 @@ def run_ours(args) -> None:
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
             "kernel": "cell_kernel (per-cell frontier transition)", "peak_source": peaks["source"],
-            "alg_bytes_per_launch": tot_bytes / (W - 1), "mean_launch_ms": tot_ms / (W - 1)}
+            "alg_bytes_per_launch": tot_bytes / (W - 1), "mean_launch_ms": tot_ms / (W - 1),
+            "row_ms": tot_ms,
+            "cell_gbs": [fdp.cell_bytes(W, p) * lanes / (cell_ms[p] * 1e-3) / 1e9 for p in range(1, W)]}
+    tuning = eng.get_tuning()
+    eng.close()  # frees the state before the sub-runs below
 
     transitions = plan.transitions_per_residue * k * args.steps * world
     line = {
         "metric": METRIC, "value": value, "unit": "residues/hour", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-        "data": "none: the DP state is generated by the row-0 initialiser",
-        "config": {"workload": f"n={n} exact count: {k} largest primes below 2^32, {lanes} residues "
-                               f"per pass, all passes in one CUDA graph", "n": n, "moduli": k, "lanes": lanes,
-                   "passes": plan.passes, "state_gib": plan.state_bytes / 2**30,
-                   "tuning": eng.get_tuning(), "autotuned": tuned["best"] if tuned else None,
-                   "l2": "state far larger than L2 (126 MB); no flush needed",
-                   "parallelism": f"replicas x{world}"},
+        "data": "none: the DP has no input data; the state is generated on the device",
+        "config": bench_config(n, k, world),
+        "plan": {"lanes": lanes, "passes": plan.passes, "state_gib": plan.state_bytes / 2**30,
+                 "tuning": tuning, "autotuned": tuned["best"] if tuned else None},
         "transitions_per_s": transitions / dev_s,
         "residues": results,
         "check": published_check(n, moduli, results),
@@ -368,40 +417,70 @@ def run_ours(args) -> None:
         "clocks": clocks,
     }
     line.update(extra)
+    if rank == 0 and world == 1 and not args.no_n20:
+        line["n20"] = run_n20(local)
+    if rank == 0 and world == 1 and not args.no_serve:
+        line["serving"] = run_serving_stream(args.seed, args.serve_requests, args.serve_gap, 0.1,
+                                             args.serve_budget_gb, args.serve_slots)
     if rank == 0 and world == 1 and not args.no_cpu:
         s = ggcount_sample()
-        v = scale_cpu(s, n)
-        line["cpu_baseline"] = {
-            "value": v, "unit": "residues/hour", "cores": s["cores"], "kind": s["kind"],
-            "sample": f"ggcount_multi -q {s['n']} %{s['modulus']} one residue in {s['seconds']:.2f} s, "
-                      f"scaled to n={n} by frontier transitions per residue"}
+        line["cpu_baseline"] = cpu_baseline_record(s, n, scale_cpu(s, n))
     if rank == 0:
         print(json.dumps(line), flush=True)
-    eng.close()
     group.close()
 
 
-def run_serving(args) -> None:
+def run_n20(device: int) -> dict:
+    """Config 2: n = 20, the four largest primes below 2^32, plain (one modulus
+    per pass, lanes = 1) and batched (one pass of four lanes); every residue is
+    checked against the reference's CPU counter (tests/golden/ggcount_residues.json)."""
+    import fdp
+    mods = primes_below_2_32(4)
+    with open(os.path.join(ROOT, "tests", "golden", "ggcount_residues.json")) as f:
+        ref = {e["modulus"]: e["residue"] for e in json.load(f)["residues"] if e["n"] == 20}
+    out = {}
+    with fdp.Engine(device) as eng:
+        for name, lanes in (("plain", 1), ("batched", 4)):
+            eng.residues(20, mods, lanes)  # warm-up: tables, capture, first touch
+            r = eng.residues(20, mods, lanes)
+            if [ref.get(m) for m in mods] != r.residues:
+                raise SystemExit(f"n=20 {name}: residues {r.residues} != ggcount {[ref.get(m) for m in mods]}")
+            out[name] = {"residues_per_hour": 3600.0 * len(mods) / r.stats.device_s, "device_s": r.stats.device_s,
+                         "lanes": lanes}
+    out["residues"] = [ref[m] for m in mods]
+    out["checked_against"] = "reference CPU counter (ggcount), tests/golden/ggcount_residues.json"
+    out["batched_over_plain"] = out["batched"]["residues_per_hour"] / out["plain"]["residues_per_hour"]
+    return out
+
+
+def run_serving_stream(seed: int, count: int, gap: float, time_scale: float, budget_gb: float,
+                       slots: int) -> dict:
     """The serving stream: seeded Poisson arrivals, n ~ U{12..21}, k ~ U{1..8}
-    largest-below-2^32 primes, admission under an HBM budget."""
+    largest-below-2^32 primes, admission under an HBM budget.  Every residue
+    is checked against the same request run alone through fdp_run_sync."""
     import random
     import threading as th
     import fdp
-    rng = random.Random(args.seed)
+    rng = random.Random(seed)
     primes = primes_below_2_32(8)
     reqs, t = [], 0.0
-    for _ in range(args.serve_requests):
-        t += rng.expovariate(1.0 / args.serve_gap)
+    for _ in range(count):
+        t += rng.expovariate(1.0 / gap)
         n = rng.randint(12, 21)
         k = rng.randint(1, 8)
-        reqs.append((t * args.serve_time_scale, n, primes[:k]))
+        reqs.append((t * time_scale, n, primes[:k]))
     eng = fdp.Engine(0)
-    # warm-up: tables and kernels for every n of the stream
+    # Warm-up (tables and kernels for every n of the stream), which also gives
+    # every request's residues alone: one run of each n with all 8 primes.
+    alone = {}
     for n in sorted({r[1] for r in reqs}):
-        eng.residues(n, primes[:1], 1)
-    eng.server_start(int(args.serve_budget_gb * 1e9), max_active=args.serve_slots, max_lanes=8)
+        alone[n] = eng.residues(n, primes, 8).residues
+    eng.close()
+    eng = fdp.Engine(0)
+    eng.server_start(int(budget_gb * 1e9), max_active=slots, max_lanes=8)
     ids = [None] * len(reqs)
     t0 = time.perf_counter()
+
     def submitter():
         for i, (at, n, mods) in enumerate(reqs):
             d = at - (time.perf_counter() - t0)
@@ -416,33 +495,44 @@ def run_serving(args) -> None:
     for i in range(len(reqs)):
         while ids[i] is None:
             time.sleep(0.001)
-        r = eng.wait(ids[i], timeout_ms=3600 * 1000)
-        results.append(r)
+        results.append(eng.wait(ids[i], timeout_ms=3600 * 1000))
     makespan = time.perf_counter() - t0
     sub.join()
     clocks = sampler.stop()
     stats = eng.server_stats()
     eng.server_stop()
+    eng.close()
+    mismatches = sum(1 for (_, n, mods), r in zip(reqs, results) if r["residues"] != alone[n][:len(mods)])
+    if mismatches:
+        raise SystemExit(f"serving: {mismatches} requests differ from the same request run alone")
     lat = sorted(r["latency_s"] for r in results)
+
     def pct(q):
         return lat[min(len(lat) - 1, int(q * len(lat)))]
     residues = sum(len(m) for _, _, m in reqs)
-    line = {
-        "metric": "serving stream latency and throughput (continuous batching)", "value": pct(0.5),
-        "unit": "s (p50 latency)", "higher_is_better": False, "n_gpus": 1, "dtype": "u32",
-        "config": {"workload": f"seed {args.seed}: {len(reqs)} requests, Poisson arrivals mean gap "
-                               f"{args.serve_gap} s x time scale {args.serve_time_scale}, n~U{{12..21}}, "
-                               f"k~U{{1..8}} largest primes below 2^32", "budget_gb": args.serve_budget_gb,
-                   "slots": args.serve_slots, "max_lanes": 8},
+    return {
+        "workload": f"seed {seed}: {len(reqs)} requests, Poisson arrivals mean gap {gap} s x time scale "
+                    f"{time_scale}, n~U{{12..21}}, k~U{{1..8}} largest primes below 2^32",
+        "budget_gb": budget_gb, "slots": slots, "max_lanes": 8,
         "p50_latency_s": pct(0.5), "p99_latency_s": pct(0.99), "max_latency_s": lat[-1],
         "mean_queue_s": statistics.mean(r["queue_s"] for r in results),
         "throughput_residues_per_hour": 3600.0 * residues / makespan,
         "throughput_requests_per_s": len(reqs) / makespan, "makespan_s": makespan,
         "peak_running": stats["peak_running"], "peak_gb_in_use": stats["peak_bytes_in_use"] / 1e9,
-        "completed": stats["completed"], "failed": stats["failed"], "clocks": clocks,
+        "completed": stats["completed"], "failed": stats["failed"],
+        "results_equal_alone": len(reqs) - mismatches, "clocks": clocks,
     }
+
+
+def run_serving(args) -> None:
+    rec = run_serving_stream(args.seed, args.serve_requests, args.serve_gap, args.serve_time_scale,
+                             args.serve_budget_gb, args.serve_slots)
+    line = {"metric": "serving stream latency and throughput (continuous batching)",
+            "value": rec["p50_latency_s"], "unit": "s (p50 latency)", "higher_is_better": False, "n_gpus": 1,
+            "dtype": "u32", "config": {"workload": rec["workload"], "budget_gb": rec["budget_gb"],
+                                       "slots": rec["slots"], "max_lanes": 8}}
+    line.update(rec)
     print(json.dumps(line), flush=True)
-    eng.close()
 
 
 def run_cells_only(args) -> None:
@@ -470,6 +560,8 @@ def main() -> None:
     ap.add_argument("--profile-rows", type=int, default=1)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-n20", action="store_true", help="skip the n=20 plain/batched sub-record")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream sub-record")
     ap.add_argument("--serve", action="store_true", help="run the serving stream instead")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--serve-requests", type=int, default=200)

@@ -265,9 +265,14 @@ fdp_status fdp_server_get_stats(fdp_ctx *ctx, fdp_server_stats *stats);
  * per candidate, median, and a known-residue check that aborts on a wrong
  * answer).  Candidates: residues per pass (how the k moduli of the problem
  * split into passes; problem->lanes is the largest allowed), one launch vs one
- * launch per lane panel, and the CTA size.  Each sample is a timed row sweep of
- * the problem's own n on the context's state buffers; the score is the
- * estimated device seconds per residue.  The winner is applied to the context
+ * launch per lane panel, and the CTA size; then, for the winner, the cell
+ * kernel's scheduling knobs one at a time (lane_items, share_min,
+ * compact_max_p, compact_items; a change is kept when the row is at least
+ * 0.5 % faster).  Each sample is a timed row sweep of the problem's own n on
+ * the context's state buffers; the score is the estimated device seconds per
+ * residue.  The known-answer check runs the tuned configuration at the
+ * problem's own n when the reference publishes a residue mod 4294967291 for
+ * it (n = 9, 18, 20, 21, 22, 23), else at n = 9.  The winner is applied to the context
  * (fdp_set_tuning) and returned; json_out (if not NULL) receives every
  * candidate record as a JSON document of at most json_cap bytes.
  */
@@ -279,6 +284,7 @@ typedef struct fdp_autotune_result {
   double s_per_residue;     /* estimated device seconds per residue              */
   double residues_per_hour; /* 3600 / s_per_residue                               */
   int candidates, rejected_memory;
+  int check_n;              /* grid size of the known-residue check            */
 } fdp_autotune_result;
 fdp_status fdp_autotune(fdp_ctx *ctx, const fdp_problem *problem, uint64_t hbm_budget_bytes, int repeats,
                         fdp_autotune_result *out, char *json_out, size_t json_cap);
@@ -302,6 +308,42 @@ fdp_status fdp_transfer_map_apply(fdp_ctx *ctx, const fdp_transfer_map *map, int
                                   const uint32_t *d_in_main, const uint32_t *d_in_block, uint32_t *d_out_main,
                                   uint32_t *d_out_block, void *stream);
 void fdp_transfer_map_destroy(fdp_transfer_map *map);
+
+/*
+ * Factorized transfer map over occupancy groups: one CSR per group shape,
+ * reused for every conjugate group (the reference's
+ * src/cuda/b300/factor_transfer_map.cuh:1-68 with its batched apply,
+ * factor_transfer_batch.cuh:13-164).  A group is the set of words (main and
+ * blocked) whose bottom `fixed` positions hold R or L exactly at the set bits
+ * of a mask and N elsewhere; cell p (and p-1 when `paired`) leaves those
+ * positions alone and its closures only swap R and L, so every group is closed
+ * under the operator, and two groups with the same number `occupied` of set
+ * bits are conjugate: moving the occupied symbols in order between the
+ * positions keeps the canonical order and every source.  The CSR is built on
+ * the device over the local ranks of the representative group (the bottom
+ * `occupied` positions set) with the count / scan / fill / check sequence of
+ * fdp_transfer_map_build; requires fixed <= p - 1 (p - 2 when paired) and
+ * fixed <= 24.  fdp_factor_map_apply runs it on `groups` (<= max_groups <= 32)
+ * groups at once for one modulus: the groups' values are gathered from the
+ * global vectors (plain layout, one residue per state) into an arena with the
+ * groups interleaved as columns, the CSR is applied column by column with one
+ * reduction per output, and the results are scattered to their global ranks
+ * in the output vectors (out_main = in_main + T x, out_block = T x on the
+ * groups' rows; other rows are not written).  masks is host memory, each with
+ * `occupied` set bits below bit `fixed`.  phase_ms (3 entries, may be NULL)
+ * receives the CUDA-event times of gather, apply and scatter, the reference's
+ * GRIDFP_PROFILE_BATCH phase timers (factor_transfer_batch.cuh:110-158); with
+ * it the call waits for the stream.
+ */
+typedef struct fdp_factor_map fdp_factor_map;
+fdp_status fdp_factor_map_build(fdp_ctx *ctx, int width, int p, int paired, int fixed, int occupied,
+                                int max_groups, fdp_factor_map **out);
+fdp_status fdp_factor_map_info(const fdp_factor_map *map, uint64_t *group_main, uint64_t *group_blocked,
+                               uint64_t *edges, uint64_t *device_bytes);
+fdp_status fdp_factor_map_apply(fdp_ctx *ctx, const fdp_factor_map *map, uint32_t modulus, int groups,
+                                const uint32_t *masks, const uint32_t *d_in_main, const uint32_t *d_in_block,
+                                uint32_t *d_out_main, uint32_t *d_out_block, void *stream, double *phase_ms);
+void fdp_factor_map_destroy(fdp_factor_map *map);
 
 /*
  * Two consecutive cells p, p-1 fused by recursive pull, out of place, without
@@ -353,6 +395,14 @@ fdp_status fdp_unrank_words(fdp_ctx *ctx, int width, const uint64_t *d_ranks, ui
 
 /* Ternary rank index on the device (src/common/ternary_rank_index.hpp:6-15). */
 fdp_status fdp_ternary_index(fdp_ctx *ctx, const uint32_t *d_codes, uint32_t *d_index, uint64_t count, void *stream);
+/*
+ * The same index through a table of every code of `chunk` symbols (chunk 4 or
+ * 7; 4^chunk entries): one table read per chunk of the code, the chunked
+ * device conversion of the reference (GRIDFP_TRIT_CHUNK, R2.cu:23-55, tested
+ * by tests/ternary_rank_index_test.cpp:7-27).  Codes of up to 16 symbols.
+ */
+fdp_status fdp_ternary_index_chunked(fdp_ctx *ctx, int chunk, const uint32_t *d_codes, uint32_t *d_index,
+                                     uint64_t count, void *stream);
 
 /*
  * Host helpers: state counts and the per-cell algorithmic byte model, the

@@ -434,6 +434,18 @@ extern "C" fdp_status fdp_ternary_index(fdp_ctx *c, const uint32_t *d_codes, uin
   return FDP_OK;
 }
 
+extern "C" fdp_status fdp_ternary_index_chunked(fdp_ctx *c, int chunk, const uint32_t *d_codes, uint32_t *d_index,
+                                                uint64_t count, void *stream) {
+  if (!c || (chunk != 4 && chunk != 7) || (count && (!d_codes || !d_index))) {
+    g_last_error = "ternary_index_chunked: chunk must be 4 or 7";
+    return FDP_ERR_ARGS;
+  }
+  FDP_CK(cudaSetDevice(c->device), "cudaSetDevice");
+  FDP_CK(fdp::launch_ternary_index_chunked(chunk, d_codes, d_index, count, stream ? (cudaStream_t)stream : c->stream),
+         "ternary chunked");
+  return FDP_OK;
+}
+
 extern "C" fdp_status fdp_time_cells(fdp_ctx *c, const fdp_problem *pr, int rows, double *cell_ms) {
   if (!c || !cell_ms || rows < 1) return FDP_ERR_ARGS;
   fdp_status s = check_problem(pr);

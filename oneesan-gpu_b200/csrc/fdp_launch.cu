@@ -389,6 +389,46 @@ cudaError_t launch_unrank_words(int width, const uint64_t *ranks, uint64_t *word
   return cudaGetLastError();
 }
 
+// Chunked conversion (the reference's GRIDFP_TRIT_CHUNK, R2.cu:23-55): a table
+// of the ternary index of every code of `CH` symbols (4^CH entries, built in
+// shared memory by each block), so a code of up to 16 symbols converts with
+// one table read per chunk: index = sum_k T[chunk_k] x (3^CH)^k.
+template <int CH>
+__global__ void ternary_index_chunked_kernel(const uint32_t *codes, uint32_t *index, uint64_t count) {
+  constexpr uint32_t n = 1u << (2 * CH), mask = n - 1u;
+  constexpr uint32_t radix = CH == 7 ? 2187u : 81u;
+  __shared__ uint16_t T[n];
+  for (uint32_t c = threadIdx.x; c < n; c += blockDim.x) {
+    uint32_t x = 0, scale = 1, v = c;
+    for (int k = 0; k < CH; ++k) {
+      x += (v & 3u) * scale;
+      scale *= 3u;
+      v >>= 2;
+    }
+    T[c] = uint16_t(x);
+  }
+  __syncthreads();
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    uint32_t c = codes[i], x = 0, scale = 1;
+    for (int off = 0; off < 16 && c; off += CH) {
+      x += uint32_t(T[c & mask]) * scale;
+      scale *= radix;
+      c >>= 2 * CH;
+    }
+    index[i] = x;
+  }
+}
+
+cudaError_t launch_ternary_index_chunked(int chunk, const uint32_t *codes, uint32_t *index, uint64_t count,
+                                         cudaStream_t s) {
+  if (chunk != 4 && chunk != 7) return cudaErrorInvalidValue;
+  if (!count) return cudaSuccess;
+  if (chunk == 4) ternary_index_chunked_kernel<4><<<grid_for(count), 256, 0, s>>>(codes, index, count);
+  else ternary_index_chunked_kernel<7><<<grid_for(count), 256, 0, s>>>(codes, index, count);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_ternary_index(const uint32_t *codes, uint32_t *index, uint64_t count, cudaStream_t s) {
   if (!count) return cudaSuccess;
   ternary_index_kernel<<<grid_for(count), 256, 0, s>>>(codes, index, count);

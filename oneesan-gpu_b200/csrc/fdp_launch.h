@@ -68,6 +68,8 @@ cudaError_t prepare_expand_tables(const std::vector<int> &caps);
 cudaError_t launch_rank_words(int width, const uint64_t *words, uint64_t *ranks, uint64_t count, cudaStream_t s);
 cudaError_t launch_unrank_words(int width, const uint64_t *ranks, uint64_t *words, uint64_t count, cudaStream_t s);
 cudaError_t launch_ternary_index(const uint32_t *codes, uint32_t *index, uint64_t count, cudaStream_t s);
+cudaError_t launch_ternary_index_chunked(int chunk, const uint32_t *codes, uint32_t *index, uint64_t count,
+                                         cudaStream_t s);
 
 int device_sm_count();
 

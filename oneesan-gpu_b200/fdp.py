@@ -63,7 +63,7 @@ class AutotuneResult(ctypes.Structure):
     _fields_ = [("lanes", ctypes.c_int), ("passes", ctypes.c_int), ("tuning", Tuning),
                 ("row_ms", ctypes.c_double), ("s_per_residue", ctypes.c_double),
                 ("residues_per_hour", ctypes.c_double), ("candidates", ctypes.c_int),
-                ("rejected_memory", ctypes.c_int)]
+                ("rejected_memory", ctypes.c_int), ("check_n", ctypes.c_int)]
 
 
 class RunStats(ctypes.Structure):
@@ -121,6 +121,12 @@ def lib() -> ctypes.CDLL:
     L.fdp_transfer_map_apply.argtypes = [c_vp, c_vp, c_int, P(c_u32), c_vp, c_vp, c_vp, c_vp, c_vp]
     L.fdp_transfer_map_destroy.argtypes = [c_vp]
     L.fdp_transfer_map_destroy.restype = None
+    L.fdp_factor_map_build.argtypes = [c_vp, c_int, c_int, c_int, c_int, c_int, c_int, P(c_vp)]
+    L.fdp_factor_map_info.argtypes = [c_vp, P(c_u64), P(c_u64), P(c_u64), P(c_u64)]
+    L.fdp_factor_map_apply.argtypes = [c_vp, c_vp, c_u32, c_int, P(c_u32), c_vp, c_vp, c_vp, c_vp, c_vp,
+                                       P(ctypes.c_double)]
+    L.fdp_factor_map_destroy.argtypes = [c_vp]
+    L.fdp_factor_map_destroy.restype = None
     L.fdp_reverse2_apply.argtypes = [c_vp, c_int, c_int, c_int, P(c_u32), c_vp, c_vp, c_vp, c_vp, c_vp]
     L.fdp_run_multi_sync.argtypes = [c_vp, P(Problem), c_int, P(c_u32), P(RunStats)]
     L.fdp_server_start.argtypes = [c_vp, P(ServerConfig)]
@@ -132,6 +138,7 @@ def lib() -> ctypes.CDLL:
     L.fdp_rank_words.argtypes = [c_vp, c_int, c_vp, c_vp, c_u64, c_vp]
     L.fdp_unrank_words.argtypes = [c_vp, c_int, c_vp, c_vp, c_u64, c_vp]
     L.fdp_ternary_index.argtypes = [c_vp, c_vp, c_vp, c_u64, c_vp]
+    L.fdp_ternary_index_chunked.argtypes = [c_vp, c_int, c_vp, c_vp, c_u64, c_vp]
     for name in ("fdp_main_states", "fdp_blocked_states"):
         getattr(L, name).argtypes = [c_int]
         getattr(L, name).restype = c_u64
@@ -352,6 +359,13 @@ class Engine:
                "fdp_transfer_map_build")
         return TransferMap(self, h)
 
+    def factor_map(self, width: int, p: int, fixed: int, occupied: int, paired: bool = False,
+                   max_groups: int = 32) -> "FactorMap":
+        h = ctypes.c_void_p()
+        _check(lib().fdp_factor_map_build(self._ctx, width, p, 1 if paired else 0, fixed, occupied, max_groups,
+                                          ctypes.byref(h)), "fdp_factor_map_build")
+        return FactorMap(self, h)
+
     def reverse2_apply(self, width: int, p: int, moduli: Sequence[int], in_main: int, in_block: int,
                        out_main: int, out_block: int, stream: int = 0) -> None:
         mods = _u32_array(moduli)
@@ -372,6 +386,10 @@ class Engine:
 
     def ternary_index(self, codes_ptr: int, index_ptr: int, count: int, stream: int = 0) -> None:
         _check(lib().fdp_ternary_index(self._ctx, codes_ptr, index_ptr, count, stream), "fdp_ternary_index")
+
+    def ternary_index_chunked(self, chunk: int, codes_ptr: int, index_ptr: int, count: int, stream: int = 0) -> None:
+        _check(lib().fdp_ternary_index_chunked(self._ctx, chunk, codes_ptr, index_ptr, count, stream),
+               "fdp_ternary_index_chunked")
 
 
 class TransferMap:
@@ -395,6 +413,40 @@ class TransferMap:
     def close(self) -> None:
         if self._h:
             lib().fdp_transfer_map_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FactorMap:
+    """A CSR over one occupancy-group shape, applied to many conjugate groups
+    (fdp_factor_map_*)."""
+
+    def __init__(self, engine: Engine, handle):
+        self._eng, self._h = engine, handle
+
+    def info(self) -> dict:
+        gm, gd, e, b = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().fdp_factor_map_info(self._h, ctypes.byref(gm), ctypes.byref(gd), ctypes.byref(e),
+                                         ctypes.byref(b)), "fdp_factor_map_info")
+        return {"group_main": gm.value, "group_blocked": gd.value, "edges": e.value, "device_bytes": b.value}
+
+    def apply(self, modulus: int, masks: Sequence[int], in_main: int, in_block: int, out_main: int,
+              out_block: int, stream: int = 0, timed: bool = False):
+        """Apply to the groups `masks`; returns [gather, apply, scatter] ms when timed."""
+        m = _u32_array(masks)
+        ph = (ctypes.c_double * 3)() if timed else None
+        _check(lib().fdp_factor_map_apply(self._eng._ctx, self._h, modulus, len(masks), m, in_main, in_block,
+                                          out_main, out_block, stream, ph), "fdp_factor_map_apply")
+        return [float(x) for x in ph] if timed else None
+
+    def close(self) -> None:
+        if self._h:
+            lib().fdp_factor_map_destroy(self._h)
             self._h = None
 
     def __del__(self):

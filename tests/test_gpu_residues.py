@@ -72,12 +72,30 @@ def test_autotune_picks_a_correct_configuration(engine):
     try:
         rec = engine.autotune(14, mods, max_lanes=6, repeats=1)
         best = rec["best"]
-        assert rec["known_residue_check"] == "ok"
+        # no published residue at n = 14: the check runs at n = 9
+        assert rec["known_residue_check"] == {"n": 9, "status": "ok"}
         assert 1 <= best["lanes"] <= 6 and best["s_per_residue"] > 0
-        assert engine.get_tuning()["block"] == best["block"]
+        tuned = engine.get_tuning()
+        for knob in ("block", "lane_items", "share_min", "compact_max_p", "compact_items"):
+            assert tuned[knob] == best[knob], knob
         assert {c["lanes"] for c in rec["candidates"]} >= {1, 2, 4, 6}
         assert engine.residues(14, mods, lanes=best["lanes"]).residues == [orc.residue(14, m) for m in mods[:1]] + \
             engine.residues(14, mods[1:], lanes=1).residues
+    finally:
+        engine.set_tuning()
+
+
+def test_autotune_checks_the_published_residue_of_its_own_n(engine):
+    # n = 18 has a published residue mod 4294967291 (503411004): the tuned
+    # configuration is checked at n = 18 itself; stage 2 tried the knobs.
+    try:
+        rec = engine.autotune(18, P[:4], max_lanes=4, repeats=1)
+        assert rec["known_residue_check"] == {"n": 18, "status": "ok"}
+        knobs = {k for c in rec["candidates"] for k in c if k in ("lane_items", "share_min", "compact_max_p",
+                                                                 "compact_items")}
+        assert knobs == {"lane_items", "share_min", "compact_max_p", "compact_items"}
+        lanes = rec["best"]["lanes"]
+        assert engine.residues(18, P[:4], lanes=lanes).residues == [503411004, 2737033518, 2864590416, 278648965]
     finally:
         engine.set_tuning()
 

@@ -6,7 +6,8 @@ the reference tree (skipped where it is absent):
   configuration from scratch_fits, dp_peak_gib and row6_peak_gib;
 * scripts/solve/solver_output.py:25-74 -- the strict result-line parser the
   exact runner uses, applied to result lines this solver printed on a B200
-  (tests/golden/solver_stdout_n9.txt)."""
+  (tests/golden/solver_stdout_n9.txt, the stdout of
+  `oneesan-gpu_b200/oneesan_solver 9 512 14 1 4294967291 4294966997 2147483647`)."""
 import importlib.util
 import os
 import subprocess

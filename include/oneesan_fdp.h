@@ -192,7 +192,10 @@ fdp_status fdp_time_cells(fdp_ctx *ctx, const fdp_problem *problem, int rows, do
  * row sweeps, when its scratch fits the blocked state buffer (0 = automatic:
  * 7 rows from width 18 up, 6 from width 14; -1 = never); row_init_product:
  * the initialiser's products on the tensor cores (0, tcgen05 with 8-bit limbs)
- * or on the CUDA cores (1).  Results never depend on these settings.
+ * or on the CUDA cores (1); split_spans_min_p: for lane counts above 8 (two
+ * spans), cells p >= split_spans_min_p run each span as its own single-span
+ * launch instead of one launch that stages closure sources (0 = the
+ * default).  Results never depend on these settings.
  */
 typedef struct fdp_tuning {
   int block;
@@ -205,6 +208,7 @@ typedef struct fdp_tuning {
   int compact_items;   /* states per lane of a grouped chunk, 0..4 (0: automatic) */
   int row_init_rows;   /* rows filled by the row-k initialiser, 2..7 (0: automatic, -1: none) */
   int row_init_product; /* its products on the tensor cores (0, default) or CUDA cores (1) */
+  int split_spans_min_p; /* cells p >= this run each lane span as its own launch (0: default) */
 } fdp_tuning;
 fdp_status fdp_set_tuning(fdp_ctx *ctx, const fdp_tuning *tuning);
 fdp_status fdp_get_tuning(fdp_ctx *ctx, fdp_tuning *tuning);
@@ -267,8 +271,8 @@ fdp_status fdp_server_get_stats(fdp_ctx *ctx, fdp_server_stats *stats);
  * split into passes; problem->lanes is the largest allowed), one launch vs one
  * launch per lane panel, and the CTA size; then, for the winner, the cell
  * kernel's scheduling knobs one at a time (lane_items, share_min,
- * compact_max_p, compact_items; a change is kept when the row is at least
- * 0.5 % faster).  Each sample is a timed row sweep of the problem's own n on
+ * compact_max_p, compact_items, and split_spans_min_p above 8 lanes; a change
+ * is kept when the row is at least 0.5 % faster).  Each sample is a timed row sweep of the problem's own n on
  * the context's state buffers; the score is the estimated device seconds per
  * residue.  The known-answer check runs the tuned configuration at the
  * problem's own n when the reference publishes a residue mod 4294967291 for

@@ -498,7 +498,8 @@ extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   if (!c || !t) return FDP_ERR_ARGS;
   if (t->block < 64 || t->block > 256 || t->block % 32 || t->grid < 0 || t->lane_items < 0 || t->lane_items > 64 ||
       t->share_min < 0 || t->compact_max_p < -1 || t->compact_items < 0 || t->compact_items > FDP_REC_MAX_ITEMS ||
-      t->row_init_rows < -1 || t->row_init_rows > 7 || t->row_init_product < 0 || t->row_init_product > 1) {
+      t->row_init_rows < -1 || t->row_init_rows > 7 || t->row_init_product < 0 || t->row_init_product > 1 ||
+      t->split_spans_min_p < 0) {
     g_last_error =
         "tuning: block must be a multiple of 32 in 64..256, grid >= 0, lane_items 0..64, share_min >= 0, "
         "compact_max_p >= -1, compact_items 0..4, row_init_rows -1..7, row_init_product 0..1";
@@ -515,6 +516,7 @@ extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   c->cfg.compact_items = t->compact_items;
   c->cfg.row_init = t->row_init_rows;
   c->cfg.row_init_tensor = t->row_init_product == 0;
+  c->cfg.split_spans_min_p = t->split_spans_min_p > 0 ? t->split_spans_min_p : fdp::LaunchCfg{}.split_spans_min_p;
   return FDP_OK;
 }
 
@@ -531,6 +533,7 @@ extern "C" fdp_status fdp_get_tuning(fdp_ctx *c, fdp_tuning *t) {
   t->compact_items = c->cfg.compact_items;
   t->row_init_rows = c->cfg.row_init;
   t->row_init_product = c->cfg.row_init_tensor ? 0 : 1;
+  t->split_spans_min_p = c->cfg.split_spans_min_p;
   return FDP_OK;
 }
 

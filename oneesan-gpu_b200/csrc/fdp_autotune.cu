@@ -9,8 +9,9 @@
 // kernel's scheduling knobs of the winner one at a time (coordinate descent,
 // a change kept only when the row is at least 0.5 % faster): the warp chunk
 // (lane_items), the shortest shared prefix decode (share_min), the highest
-// cell updated grouped by centre type (compact_max_p) and the states per lane
-// of a grouped chunk (compact_items).
+// cell updated grouped by centre type (compact_max_p), the states per lane
+// of a grouped chunk (compact_items) and, for lane counts above 8, the lowest
+// cell that runs each lane span as its own launch (split_spans_min_p).
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -153,7 +154,8 @@ extern "C" fdp_status fdp_autotune(fdp_ctx *c, const fdp_problem *pr, uint64_t b
   const Knob knobs[] = {{"lane_items", &fdp_tuning::lane_items, {4, 8, 16}},
                         {"share_min", &fdp_tuning::share_min, {2, 4, 6}},
                         {"compact_max_p", &fdp_tuning::compact_max_p, {5, 7, 9}},
-                        {"compact_items", &fdp_tuning::compact_items, {1, 2, 4}}};
+                        {"compact_items", &fdp_tuning::compact_items, {1, 2, 4}},
+                        {"split_spans_min_p", &fdp_tuning::split_spans_min_p, {8, 12}}};
   {
     fdp_problem cand{pr->n, best.lanes, pr->moduli, best.lanes};
     fdp_tuning cur{};
@@ -163,6 +165,8 @@ extern "C" fdp_status fdp_autotune(fdp_ctx *c, const fdp_problem *pr, uint64_t b
     fdp_plan(&cand, budget, &plan);
     const int swept = rows - (plan.init_rows >= 2 ? plan.init_rows - 1 : 0);
     for (const Knob &kb : knobs) {
+      // Span splitting only applies to lane counts of two spans (above 8).
+      if (kb.field == &fdp_tuning::split_spans_min_p && best.lanes <= 8) continue;
       const int keep = cur.*kb.field;
       for (int v : kb.values) {
         if (s != FDP_OK || v == keep) continue;
@@ -224,10 +228,11 @@ extern "C" fdp_status fdp_autotune(fdp_ctx *c, const fdp_problem *pr, uint64_t b
   char tail[512];
   snprintf(tail, sizeof(tail),
            "],\"best\":{\"lanes\":%d,\"passes\":%d,\"split_panels\":%d,\"block\":%d,\"lane_items\":%d,"
-           "\"share_min\":%d,\"compact_max_p\":%d,\"compact_items\":%d,\"row_ms\":%.4f,"
+           "\"share_min\":%d,\"compact_max_p\":%d,\"compact_items\":%d,\"split_spans_min_p\":%d,\"row_ms\":%.4f,"
            "\"s_per_residue\":%.6f,\"residues_per_hour\":%.3f},\"known_residue_check\":{\"n\":%d,\"status\":\"ok\"}}",
            best.lanes, best.passes, best.tuning.split_panels, best.tuning.block, best.tuning.lane_items,
-           best.tuning.share_min, best.tuning.compact_max_p, best.tuning.compact_items, best.row_ms,
+           best.tuning.share_min, best.tuning.compact_max_p, best.tuning.compact_items,
+           best.tuning.split_spans_min_p, best.row_ms,
            best.s_per_residue, best.residues_per_hour, best.check_n);
   js += tail;
   if (json_out && json_cap) {

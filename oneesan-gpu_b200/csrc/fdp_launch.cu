@@ -97,6 +97,23 @@ cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_
     if (a.lane_items > most) a.lane_items = most;
   }
   const bool one_panel = (K == 1 || K == 2 || K == 4 || K == 8);
+  if (K > 8 && p >= cfg.split_spans_min_p && !cfg.split_panels) {
+    // Each span (panels of at most 8 lanes together) is laid out exactly as a
+    // lane count of its own width at its first panel's offset, so it runs as
+    // an independent single-span problem: one launch per span, each decoding
+    // the items again but streaming one span without staged closure sources.
+    for (int l0 = 0; l0 < K;) {
+      const int le = span_end_of(K, l0);
+      CellArgs b = a;
+      b.main = main + size_t(l0) * a.mstates;
+      b.blk = blk + size_t(l0) * a.items;
+      for (int i = 0; i < le - l0; ++i) b.mod[i] = mods[l0 + i];
+      cudaError_t e = launch_cell_k(t, le - l0, b, cfg, s);
+      if (e != cudaSuccess) return e;
+      l0 = le;
+    }
+    return cudaSuccess;
+  }
   if (one_panel || !cfg.split_panels) return launch_cell_k(t, K, a, cfg, s);
   // Every panel is an independent [N][PW] array: run each as its own K = PW problem.
   for (int l0 = 0; l0 < K;) {

@@ -34,6 +34,7 @@ struct LaunchCfg {
                              // one span, 2 when closure sources are staged, which leaves L1 room)
   int row_init = 0;          // strip rows filled directly by the row-k initialiser (0: automatic, -1: never)
   bool row_init_tensor = true;  // the initialiser's products on the tensor cores (else the CUDA cores)
+  int split_spans_min_p = 1000; // cells p >= this run each span of a several-span lane count as its own launch
 };
 
 template <typename Idx, int K>

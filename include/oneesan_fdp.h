@@ -184,8 +184,8 @@ fdp_status fdp_time_cells(fdp_ctx *ctx, const fdp_problem *problem, int rows, do
  * cells p <= compact_max_p, where the items of one warp mix centre types,
  * decode a chunk's items first and update them grouped by type (0 = the
  * default, 7; -1 = never); compact_items: states per lane of such a cell's
- * chunks, 1..4 (0 = automatic: 4 when the lanes fit one span of 8, else 2,
- * which leaves more of the SM's on-chip memory to L1); row_init_rows: the
+ * chunks (0 = automatic: without carry-over 4 when the lanes fit one span of
+ * 8, else 2, which leaves more of the SM's on-chip memory to L1); row_init_rows: the
  * pass starts from the state after the first row_init_rows rows of vertices,
  * computed directly by the row-k initialiser (a column automaton of that
  * strip, the reference's row-5/row-6 initialisers, GB.cu:874-1032) instead of
@@ -195,7 +195,13 @@ fdp_status fdp_time_cells(fdp_ctx *ctx, const fdp_problem *problem, int rows, do
  * or on the CUDA cores (1); split_spans_min_p: for lane counts above 8 (two
  * spans), cells p >= split_spans_min_p run each span as its own single-span
  * launch instead of one launch that stages closure sources (0 = the
- * default).  Results never depend on these settings.
+ * default, 1: every cell; a value above the width never splits); compact_carry: the grouped cells keep the heads of one type that
+ * do not fill a warp queued for the warp's next chunk, so every grouped
+ * update runs on 32 items (1 = on, -1 = group each chunk alone, 0 = automatic:
+ * on when the lanes fit one span of 8, the case where it was measured
+ * faster); with carry-over compact_items may be 1..16 (0 = 16) and only sets
+ * the chunk whose prefix decode is shared; without it values above 4 count
+ * as 4.  Results never depend on these settings.
  */
 typedef struct fdp_tuning {
   int block;
@@ -205,10 +211,11 @@ typedef struct fdp_tuning {
   int lane_items;      /* states per lane of a warp chunk, 0..64 (0: default)   */
   int share_min;       /* shortest prefix decoded once per chunk (0: default)   */
   int compact_max_p;   /* highest cell grouped by centre type (0: default, -1: none) */
-  int compact_items;   /* states per lane of a grouped chunk, 0..4 (0: automatic) */
+  int compact_items;   /* states per lane of a grouped chunk, 0..16 (0: automatic) */
   int row_init_rows;   /* rows filled by the row-k initialiser, 2..7 (0: automatic, -1: none) */
   int row_init_product; /* its products on the tensor cores (0, default) or CUDA cores (1) */
   int split_spans_min_p; /* cells p >= this run each lane span as its own launch (0: default) */
+  int compact_carry;   /* grouped cells queue heads across chunks: 1 on, -1 off, 0 automatic */
 } fdp_tuning;
 fdp_status fdp_set_tuning(fdp_ctx *ctx, const fdp_tuning *tuning);
 fdp_status fdp_get_tuning(fdp_ctx *ctx, fdp_tuning *tuning);
@@ -271,7 +278,7 @@ fdp_status fdp_server_get_stats(fdp_ctx *ctx, fdp_server_stats *stats);
  * split into passes; problem->lanes is the largest allowed), one launch vs one
  * launch per lane panel, and the CTA size; then, for the winner, the cell
  * kernel's scheduling knobs one at a time (lane_items, share_min,
- * compact_max_p, compact_items, and split_spans_min_p above 8 lanes; a change
+ * compact_max_p, compact_carry, compact_items, and split_spans_min_p above 8 lanes; a change
  * is kept when the row is at least 0.5 % faster).  Each sample is a timed row sweep of the problem's own n on
  * the context's state buffers; the score is the estimated device seconds per
  * residue.  The known-answer check runs the tuned configuration at the

@@ -497,12 +497,15 @@ void fdp_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   if (!c || !t) return FDP_ERR_ARGS;
   if (t->block < 64 || t->block > 256 || t->block % 32 || t->grid < 0 || t->lane_items < 0 || t->lane_items > 64 ||
-      t->share_min < 0 || t->compact_max_p < -1 || t->compact_items < 0 || t->compact_items > FDP_REC_MAX_ITEMS ||
+      t->share_min < 0 || t->compact_max_p < -1 || t->compact_carry < -1 || t->compact_carry > 1 ||
+      t->compact_items < 0 || t->compact_items > (t->compact_carry < 0 ? FDP_REC_MAX_ITEMS : 16) ||
       t->row_init_rows < -1 || t->row_init_rows > 7 || t->row_init_product < 0 || t->row_init_product > 1 ||
       t->split_spans_min_p < 0) {
     g_last_error =
         "tuning: block must be a multiple of 32 in 64..256, grid >= 0, lane_items 0..64, share_min >= 0, "
-        "compact_max_p >= -1, compact_items 0..4, row_init_rows -1..7, row_init_product 0..1";
+        "compact_max_p >= -1, compact_carry -1..1, compact_items 0..16 (0..4 with compact_carry -1; "
+        "a value above 4 is used only where heads carry over), "
+        "row_init_rows -1..7, row_init_product 0..1";
     return FDP_ERR_ARGS;
   }
   std::lock_guard<std::mutex> lk(c->mu);
@@ -514,6 +517,7 @@ extern "C" fdp_status fdp_set_tuning(fdp_ctx *c, const fdp_tuning *t) {
   c->cfg.share_min = t->share_min > 0 ? t->share_min : fdp::LaunchCfg{}.share_min;
   c->cfg.compact_max_p = t->compact_max_p != 0 ? t->compact_max_p : fdp::LaunchCfg{}.compact_max_p;
   c->cfg.compact_items = t->compact_items;
+  c->cfg.compact_carry = t->compact_carry;
   c->cfg.row_init = t->row_init_rows;
   c->cfg.row_init_tensor = t->row_init_product == 0;
   c->cfg.split_spans_min_p = t->split_spans_min_p > 0 ? t->split_spans_min_p : fdp::LaunchCfg{}.split_spans_min_p;
@@ -531,6 +535,7 @@ extern "C" fdp_status fdp_get_tuning(fdp_ctx *c, fdp_tuning *t) {
   t->share_min = c->cfg.share_min;
   t->compact_max_p = c->cfg.compact_max_p;
   t->compact_items = c->cfg.compact_items;
+  t->compact_carry = c->cfg.compact_carry;
   t->row_init_rows = c->cfg.row_init;
   t->row_init_product = c->cfg.row_init_tensor ? 0 : 1;
   t->split_spans_min_p = c->cfg.split_spans_min_p;

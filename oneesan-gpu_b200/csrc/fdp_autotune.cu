@@ -9,8 +9,9 @@
 // kernel's scheduling knobs of the winner one at a time (coordinate descent,
 // a change kept only when the row is at least 0.5 % faster): the warp chunk
 // (lane_items), the shortest shared prefix decode (share_min), the highest
-// cell updated grouped by centre type (compact_max_p), the states per lane
-// of a grouped chunk (compact_items) and, for lane counts above 8, the lowest
+// cell updated grouped by centre type (compact_max_p), whether grouped heads
+// carry over between chunks (compact_carry), the states per lane of a grouped
+// chunk (compact_items) and, for lane counts above 8, the lowest
 // cell that runs each lane span as its own launch (split_spans_min_p).
 #include <math.h>
 #include <stdio.h>
@@ -154,8 +155,9 @@ extern "C" fdp_status fdp_autotune(fdp_ctx *c, const fdp_problem *pr, uint64_t b
   const Knob knobs[] = {{"lane_items", &fdp_tuning::lane_items, {4, 8, 16}},
                         {"share_min", &fdp_tuning::share_min, {2, 4, 6}},
                         {"compact_max_p", &fdp_tuning::compact_max_p, {5, 7, 9}},
-                        {"compact_items", &fdp_tuning::compact_items, {1, 2, 4}},
-                        {"split_spans_min_p", &fdp_tuning::split_spans_min_p, {8, 12}}};
+                        {"compact_carry", &fdp_tuning::compact_carry, {-1, 1}},
+                        {"compact_items", &fdp_tuning::compact_items, {1, 2, 4, 8}},
+                        {"split_spans_min_p", &fdp_tuning::split_spans_min_p, {1, 8, 1000}}};
   {
     fdp_problem cand{pr->n, best.lanes, pr->moduli, best.lanes};
     fdp_tuning cur{};
@@ -228,10 +230,11 @@ extern "C" fdp_status fdp_autotune(fdp_ctx *c, const fdp_problem *pr, uint64_t b
   char tail[512];
   snprintf(tail, sizeof(tail),
            "],\"best\":{\"lanes\":%d,\"passes\":%d,\"split_panels\":%d,\"block\":%d,\"lane_items\":%d,"
-           "\"share_min\":%d,\"compact_max_p\":%d,\"compact_items\":%d,\"split_spans_min_p\":%d,\"row_ms\":%.4f,"
+           "\"share_min\":%d,\"compact_max_p\":%d,\"compact_carry\":%d,\"compact_items\":%d,"
+           "\"split_spans_min_p\":%d,\"row_ms\":%.4f,"
            "\"s_per_residue\":%.6f,\"residues_per_hour\":%.3f},\"known_residue_check\":{\"n\":%d,\"status\":\"ok\"}}",
            best.lanes, best.passes, best.tuning.split_panels, best.tuning.block, best.tuning.lane_items,
-           best.tuning.share_min, best.tuning.compact_max_p, best.tuning.compact_items,
+           best.tuning.share_min, best.tuning.compact_max_p, best.tuning.compact_carry, best.tuning.compact_items,
            best.tuning.split_spans_min_p, best.row_ms,
            best.s_per_residue, best.residues_per_hour, best.check_n);
   js += tail;

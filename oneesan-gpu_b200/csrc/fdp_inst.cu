@@ -1,6 +1,7 @@
 // Explicit instantiations of the cell / first-row kernels for K in
 // [FDP_K_LO, FDP_K_HI]; the build compiles this file once per K range so the
 // 2 x 16 kernel variants build in parallel.
+#include <map>
 #include <mutex>
 
 #include "fdp_kernels.cuh"
@@ -16,15 +17,14 @@
 namespace fdp {
 
 // Per-device launch state of one kernel variant: the dynamic shared-memory
-// limit is raised once per device to the largest record store of the largest
-// CTA, and the occupancy of every (CTA size, record size) is resolved on first
-// use on that device.
+// limit is raised once per device to the largest layout of the largest CTA,
+// and the occupancy of every (CTA size, shared-memory size) is resolved on
+// first use on that device.
 constexpr int kInstMaxDevices = 64;
-constexpr int kBlockSizes = 256 / 32;  // CTA sizes 32 .. 256 in steps of 32
 
 struct VariantState {
   bool limit_set = false;
-  int per_sm[kBlockSizes + 1][FDP_REC_MAX_ITEMS + 1] = {};  // 0: not resolved yet
+  std::map<uint64_t, int> per_sm;  // (block, dynamic shared bytes) -> resident CTAs per SM
 };
 
 template <typename Idx, int K>
@@ -32,8 +32,9 @@ cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t 
   static std::mutex mu;
   static VariantState state[kInstMaxDevices];
   if (cfg.block < 32 || cfg.block > 256 || cfg.block % 32) return cudaErrorInvalidValue;
-  const int rec_items = a.compact ? a.lane_items : 0;  // <= FDP_REC_MAX_ITEMS (launch_cell)
-  const size_t smem = cell_smem_bytes<Idx, K>(cfg.block, rec_items);
+  if (a.W < 2 || a.W > FDP_MAXW) return cudaErrorInvalidValue;
+  const int compact = a.compact == 2 ? 2 : (a.compact && a.lane_items <= FDP_REC_MAX_ITEMS ? 1 : 0);
+  const size_t smem = cell_smem_bytes<Idx, K>(cfg.block, a.W, compact, a.lane_items);
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -43,12 +44,14 @@ cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t 
     std::lock_guard<std::mutex> lk(mu);
     VariantState &v = state[dev];
     if (!v.limit_set) {
-      const size_t most = cell_smem_bytes<Idx, K>(256, FDP_REC_MAX_ITEMS);
+      size_t most = cell_smem_bytes<Idx, K>(256, FDP_MAXW, 1, FDP_REC_MAX_ITEMS);
+      const size_t carry = cell_smem_bytes<Idx, K>(256, FDP_MAXW, 2, 0);
+      if (carry > most) most = carry;
       e = cudaFuncSetAttribute(cell_kernel<Idx, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(most));
       if (e != cudaSuccess) return e;
       v.limit_set = true;
     }
-    int &slot = v.per_sm[cfg.block / 32][rec_items];
+    int &slot = v.per_sm[(uint64_t(cfg.block) << 32) | uint64_t(smem)];
     if (slot == 0) {
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&slot, cell_kernel<Idx, K>, cfg.block, smem);
       if (e != cudaSuccess) {

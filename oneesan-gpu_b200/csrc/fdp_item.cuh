@@ -30,6 +30,13 @@
 
 namespace fdp {
 
+// Closure predecessors of one c = N target at width W: LL sources are the
+// depth-1 L's of the low word (p - 1 symbols), RR sources the depth-1 R's of
+// the high part (W - 1 - p symbols); consecutive depth-1 symbols of one kind
+// are separated by a symbol of the other kind, so there are at most
+// ceil((p-1)/2) + ceil((W-1-p)/2) <= W/2 of them.  One slot of margin.
+FDP_HD constexpr int cand_slots(int W) { return W / 2 + 1; }
+
 struct CellArgs {
   const void *tables;  // WidthTables<Idx> in device memory
   uint32_t *main;      // K lanes of M states (panel layout)
@@ -43,7 +50,8 @@ struct CellArgs {
   int cap;             // height cap of the state space (FDP_FULL_CAP: unbounded)
   int lane_items;      // items per lane of one warp chunk (the chunk is 32 * lane_items indices)
   int share_prefix;    // decode the prefix a warp chunk shares once per chunk
-  int compact;         // update a chunk's items grouped by centre type (lane_items <= FDP_REC_MAX_ITEMS)
+  int compact;         // small-p cells: 1 = a chunk's items updated grouped by centre type
+                       // (lane_items <= FDP_REC_MAX_ITEMS), 2 = grouped with carry-over queues
 };
 
 struct FirstRowArgs {
@@ -363,17 +371,31 @@ FDP_HD void apply_x(const CellArgs &a, const Idx iA, const Idx iB, const Idx j) 
   }
 }
 
+// The two main words of a c = R/L head: the owned NR/NL word and the RN/LN
+// source (item_x's operands).
+template <typename Idx>
+FDP_HD void x_words(const CellSmem<Idx> &sm, const Head<Idx> &hd, Idx &ia, Idx &ib) {
+  const Idx *off = sm.OFF[hd.h];
+  ia = hd.bm + off[hd.c == 1 ? PR_NR : PR_NL] + hd.r;
+  ib = hd.bm + off[hd.c == 1 ? PR_RN : PR_LN] + hd.r;
+}
+
 template <typename Idx, int K>
 FDP_HD void item_x(const CellArgs &a, const CellSmem<Idx> &sm, const Head<Idx> &hd) {
-  const Idx *off = sm.OFF[hd.h];
-  apply_x<Idx, K>(a, hd.bm + off[hd.c == 1 ? PR_NR : PR_NL] + hd.r, hd.bm + off[hd.c == 1 ? PR_RN : PR_LN] + hd.r,
-                  hd.j);
+  Idx ia, ib;
+  x_words<Idx>(sm, hd, ia, ib);
+  apply_x<Idx, K>(a, ia, ib, hd.j);
 }
 
 // c = N with the closure sources staged in cand[i * cstride], one span at a
-// time (streamed words first, closure sources last):
+// time:
 //   p >= 2:  NN' = NN + B, LR' = LR + NN, B' = RL + closures
 //   p == 1:  NN' = NN + B + RR closures, LR' = LR + NN, B' = 0 if stored
+// The three streamed words NN, LR and B are loaded before the first store: a
+// load placed after a store cannot be moved above it (the compiler must
+// assume they may alias), so this order costs one memory round trip where
+// load / store / load costs two.  RL and the closure sources follow, two at a
+// time.  None of those words is written by another item of the cell.
 template <typename Idx, int K, int L0 = 0>
 FDP_HD void apply_n(const CellArgs &a, const NItem<Idx> &it, const Idx *cand, int cstride) {
   if constexpr (L0 < K) {
@@ -384,17 +406,20 @@ FDP_HD void apply_n(const CellArgs &a, const NItem<Idx> &it, const Idx *cand, in
     const uint32_t *mod = a.mod + L0;
     const size_t jj = size_t(it.j);
     uint32_t x[G], acc[G];
-    ld_span<K, L0, LE>(Mn, M, size_t(it.iNN), x);
-    if (it.hasLR) {
-      uint32_t y[G];
-      ld_span<K, L0, LE>(Mn, M, size_t(it.iLR), y);
+    {
+      uint32_t y[G], b[G];
+      ld_span<K, L0, LE>(Mn, M, size_t(it.iNN), x);
+      if (!a.blk_in_zero) ld_span<K, L0, LE>(Bk, D, jj, b);
+      else {
 #pragma unroll
-      for (int i = 0; i < G; ++i) y[i] = add_mod(y[i], x[i], mod[i]);
-      st_span<K, L0, LE>(Mn, M, size_t(it.iLR), y);
-    }
-    if (!a.blk_in_zero) {
-      uint32_t b[G];
-      ld_span<K, L0, LE>(Bk, D, jj, b);
+        for (int i = 0; i < G; ++i) b[i] = 0;
+      }
+      if (it.hasLR) ld_span<K, L0, LE>(Mn, M, size_t(it.iLR), y);
+      if (it.hasLR) {
+#pragma unroll
+        for (int i = 0; i < G; ++i) y[i] = add_mod(y[i], x[i], mod[i]);
+        st_span<K, L0, LE>(Mn, M, size_t(it.iLR), y);
+      }
 #pragma unroll
       for (int i = 0; i < G; ++i) x[i] = add_mod(x[i], b[i], mod[i]);
     }
@@ -439,8 +464,8 @@ FDP_HD void apply_n(const CellArgs &a, const NItem<Idx> &it, const Idx *cand, in
 template <int K>
 FDP_HD constexpr bool stages_candidates() { return span_count<K>() > 1; }
 
-// c = N, one span (K <= 8): update the streamed words first, then add the
-// closure sources as the scans find them (same formulas as apply_n).
+// c = N, one span (K <= 8): same formulas and load order as apply_n; the
+// closure sources are added as the scans find them.
 template <typename Idx, int K>
 FDP_HD void item_n_one_span(const CellArgs &a, const CellSmem<Idx> &sm, const Head<Idx> &hd) {
   const int p = a.p;
@@ -450,19 +475,23 @@ FDP_HD void item_n_one_span(const CellArgs &a, const CellSmem<Idx> &sm, const He
   const uint32_t *mod = a.mod;
   const Idx *off = sm.OFF[hd.h];
   const Idx iNN = hd.bm + off[PR_NN] + hd.r;
-  const Idx iLR = hd.bm + off[PR_LR] + hd.r;
   uint32_t x[K], acc[K];
-  ld_span<K, 0, K>(Mn, M, size_t(iNN), x);
-  if (hd.h + 1 <= a.cap) {  // the LR target exists below the height cap
-    uint32_t y[K];
-    ld_span<K, 0, K>(Mn, M, size_t(iLR), y);
+  {
+    const Idx iLR = hd.bm + off[PR_LR] + hd.r;
+    const bool lr = hd.h + 1 <= a.cap;  // the LR target exists below the height cap
+    uint32_t y[K], b[K];
+    ld_span<K, 0, K>(Mn, M, size_t(iNN), x);
+    if (!a.blk_in_zero) ld_span<K, 0, K>(Bk, D, size_t(hd.j), b);
+    else {
 #pragma unroll
-    for (int i = 0; i < K; ++i) y[i] = add_mod(y[i], x[i], mod[i]);
-    st_span<K, 0, K>(Mn, M, size_t(iLR), y);
-  }
-  if (!a.blk_in_zero) {
-    uint32_t b[K];
-    ld_span<K, 0, K>(Bk, D, size_t(hd.j), b);
+      for (int i = 0; i < K; ++i) b[i] = 0;
+    }
+    if (lr) ld_span<K, 0, K>(Mn, M, size_t(iLR), y);
+    if (lr) {
+#pragma unroll
+      for (int i = 0; i < K; ++i) y[i] = add_mod(y[i], x[i], mod[i]);
+      st_span<K, 0, K>(Mn, M, size_t(iLR), y);
+    }
 #pragma unroll
     for (int i = 0; i < K; ++i) x[i] = add_mod(x[i], b[i], mod[i]);
   }
@@ -540,6 +569,43 @@ struct HeadRecs {
   FDP_HD Head<Idx> get(int k) const {
     const uint32_t v = hc()[k];
     return Head<Idx>{idx(0)[k], idx(1)[k], idx(2)[k], hw()[k], int(v & 255u), int(v >> 8)};
+  }
+};
+
+// Carry-over stores of the grouped small-p path, one per warp.  Heads decoded
+// from successive chunks queue by centre type until 32 of one type wait, so
+// every grouped update runs on a full warp (grouping per chunk alone leaves a
+// third of the lanes idle at p <= 6).  Each queue is a stack of at most 63
+// entries (31 carried over + 32 new): c = R/L items as their three word
+// indices, c = N items as heads with the end height packed above the high
+// symbols (at most 2 x 26 bits for W <= 28, p >= 1).
+#define FDP_CARRY_CAP 64
+template <typename Idx>
+FDP_HD constexpr size_t carry_rec_bytes() {
+  return size_t(FDP_CARRY_CAP) * (sizeof(uint64_t) + 6 * sizeof(Idx));
+}
+
+template <typename Idx>
+struct CarryRecs {
+  unsigned char *base;  // hwh[64] (u64), then x: a[64], b[64], j[64]; n: j[64], r[64], bm[64] (Idx)
+  FDP_HD uint64_t *hwh() const { return reinterpret_cast<uint64_t *>(base); }
+  FDP_HD Idx *f(int field) const {
+    return reinterpret_cast<Idx *>(base + size_t(FDP_CARRY_CAP) * 8) + field * FDP_CARRY_CAP;
+  }
+  FDP_HD void put_x(int k, Idx ia, Idx ib, Idx j) const {
+    f(0)[k] = ia;
+    f(1)[k] = ib;
+    f(2)[k] = j;
+  }
+  FDP_HD void put_n(int k, const Head<Idx> &h) const {
+    hwh()[k] = h.hw | (uint64_t(h.h) << 56);
+    f(3)[k] = h.j;
+    f(4)[k] = h.r;
+    f(5)[k] = h.bm;
+  }
+  FDP_HD Head<Idx> get_n(int k) const {
+    const uint64_t v = hwh()[k];
+    return Head<Idx>{f(3)[k], f(4)[k], f(5)[k], v & ((1ull << 56) - 1ull), int(v >> 56), 0};
   }
 };
 

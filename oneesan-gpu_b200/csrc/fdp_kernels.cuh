@@ -23,22 +23,36 @@ __device__ __forceinline__ void load_cell_smem(CellSmem<Idx> &sm, const WidthTab
 }
 
 // Dynamic shared memory of the cell kernel: the width tables, the
-// closure-candidate slots (slot i of thread t at cand[i * blockDim + t]), then
-// (compacted launches) one head-record store per warp.
+// closure-candidate slots (slot i of thread t at cand[i * blockDim + t],
+// cand_slots(W) slots), then (grouped small-p launches) one head store per
+// warp: rec_items states per lane (compact = 1) or the carry-over queues
+// (compact = 2).
 template <typename Idx, int K>
-FDP_HD constexpr size_t cell_recs_offset(int block) {
-  return (sizeof(CellSmem<Idx>) + (stages_candidates<K>() ? size_t(FDP_MAX_CAND) * block * sizeof(Idx) : 0) + 15) &
+FDP_HD constexpr size_t cell_recs_offset(int block, int W) {
+  return (sizeof(CellSmem<Idx>) + (stages_candidates<K>() ? size_t(cand_slots(W)) * block * sizeof(Idx) : 0) +
+          15) &
          ~size_t(15);
 }
 
-// rec_items: states per lane of a compacted chunk (0: not compacted).
-template <typename Idx, int K>
-FDP_HD constexpr size_t cell_smem_bytes(int block, int rec_items) {
-  return cell_recs_offset<Idx, K>(block) + size_t(block / 32) * size_t(32 * rec_items) * head_rec_entry_bytes<Idx>();
+template <typename Idx>
+FDP_HD constexpr size_t cell_recs_per_warp(int compact, int rec_items) {
+  return compact == 2 ? carry_rec_bytes<Idx>()
+                      : (compact == 1 ? size_t(32 * rec_items) * head_rec_entry_bytes<Idx>() : size_t(0));
 }
 
 template <typename Idx, int K>
-__global__ void __launch_bounds__(256, 4) cell_kernel(const CellArgs a) {
+FDP_HD constexpr size_t cell_smem_bytes(int block, int W, int compact, int rec_items) {
+  return cell_recs_offset<Idx, K>(block, W) + size_t(block / 32) * cell_recs_per_warp<Idx>(compact, rec_items);
+}
+
+// Resident CTAs of 256 threads per SM the cell kernel is compiled for (the
+// register budget per thread is 65536 / (256 x this)).
+#ifndef FDP_CELL_MIN_BLOCKS
+#define FDP_CELL_MIN_BLOCKS 4
+#endif
+
+template <typename Idx, int K>
+__global__ void __launch_bounds__(256, FDP_CELL_MIN_BLOCKS) cell_kernel(const CellArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CellSmem<Idx> &sm = *reinterpret_cast<CellSmem<Idx> *>(smem_raw);
   Idx *cand = reinterpret_cast<Idx *>(smem_raw + sizeof(CellSmem<Idx>));
@@ -59,19 +73,21 @@ __global__ void __launch_bounds__(256, 4) cell_kernel(const CellArgs a) {
   // the front and c = N from the back, so each update runs on whole warps
   // instead of two half-empty branches.  Any order of items within a cell is
   // valid: no item reads or writes a word another item writes.
-  const bool compact = a.compact && a.lane_items <= FDP_REC_MAX_ITEMS;
-  const HeadRecs<Idx> rec{smem_raw + cell_recs_offset<Idx, K>(blockDim.x) +
-                              size_t(threadIdx.x >> 5) * size_t(chunk) * head_rec_entry_bytes<Idx>(),
-                          int(chunk)};
+  const int compact = a.compact == 2 ? 2 : (a.compact && a.lane_items <= FDP_REC_MAX_ITEMS ? 1 : 0);
+  unsigned char *const recs = smem_raw + cell_recs_offset<Idx, K>(blockDim.x, a.W) +
+                              size_t(threadIdx.x >> 5) * cell_recs_per_warp<Idx>(compact, a.lane_items);
+  const HeadRecs<Idx> rec{recs, int(chunk)};
+  const CarryRecs<Idx> cr{recs};
+  int qx = 0, qn = 0;  // carry-over queue depths (warp-uniform)
   const unsigned below = (1u << (threadIdx.x & 31)) - 1u;
   for (Idx jb = (Idx(blockIdx.x) * wpb + Idx(threadIdx.x >> 5)) * chunk; jb < n; jb += step) {
     const Idx jl = (n - jb > chunk) ? jb + chunk - 1 : n - 1;
     const Prefix<Idx> pf = a.share_prefix ? shared_prefix<Idx>(a, sm, jb, jl) : empty_prefix<Idx>(a);
-    if (!compact) {
+    const Idx span = jl - jb;
+    if (compact == 0) {
       for (Idx j = jb + lane; j <= jl; j += 32) cell_item<Idx, K>(a, sm, j, pf, cand + threadIdx.x, int(blockDim.x));
-    } else {
+    } else if (compact == 1) {
       const int last = int(chunk) - 1;
-      const Idx span = jl - jb;
       int nx = 0, nn = 0;
       for (int i = 0; i < a.lane_items; ++i) {
         const Idx o = lane + Idx(32 * i);
@@ -90,9 +106,43 @@ __global__ void __launch_bounds__(256, 4) cell_kernel(const CellArgs a) {
       for (int k = int(lane); k < nn; k += 32)
         item_n<Idx, K>(a, sm, rec.get(last - k), cand + threadIdx.x, int(blockDim.x));
       __syncwarp();
+    } else {
+      // Carry-over: push one head per lane, then update 32 items of a type as
+      // soon as 32 wait; the rest stay queued for the next chunk.  Each queue
+      // holds at most 31 + 32 entries.
+      for (int i = 0; i < a.lane_items; ++i) {
+        const Idx o = lane + Idx(32 * i);
+        const bool valid = o <= span;
+        Head<Idx> hd{};
+        if (valid) hd = decode_head<Idx>(a, sm, jb + o, pf);
+        const bool isx = valid && hd.c != 0, isn = valid && hd.c == 0;
+        const unsigned bx = __ballot_sync(0xffffffffu, isx), bn = __ballot_sync(0xffffffffu, isn);
+        if (isx) {
+          Idx ia, ib;
+          x_words<Idx>(sm, hd, ia, ib);
+          cr.put_x(qx + __popc(bx & below), ia, ib, hd.j);
+        }
+        if (isn) cr.put_n(qn + __popc(bn & below), hd);
+        qx += __popc(bx);
+        qn += __popc(bn);
+        __syncwarp();
+        if (qx >= 32) {
+          qx -= 32;
+          const int k = qx + int(lane);
+          apply_x<Idx, K>(a, cr.f(0)[k], cr.f(1)[k], cr.f(2)[k]);
+        }
+        if (qn >= 32) {
+          qn -= 32;
+          item_n<Idx, K>(a, sm, cr.get_n(qn + int(lane)), cand + threadIdx.x, int(blockDim.x));
+        }
+        __syncwarp();
+      }
     }
     if (n - jb <= step) break;  // the next chunk start would be past n (and may wrap)
   }
+  // Whatever the carry-over queues still hold.
+  if (int(lane) < qx) apply_x<Idx, K>(a, cr.f(0)[lane], cr.f(1)[lane], cr.f(2)[lane]);
+  if (int(lane) < qn) item_n<Idx, K>(a, sm, cr.get_n(int(lane)), cand + threadIdx.x, int(blockDim.x));
 }
 
 template <typename Idx, int K>

@@ -60,7 +60,34 @@ void free_tables(DevTables *t) {
     default: return cudaErrorInvalidValue; \
   }
 
-static cudaError_t launch_cell_k(const DevTables &t, int K, const CellArgs &a, const LaunchCfg &cfg, cudaStream_t s) {
+// The scheduling fields of the launch for K lanes (after any split into
+// spans or panels): warp chunk, and for small p grouping by centre type,
+// with or without carry-over.
+static CellArgs schedule_cell(const CellArgs &in, int K, const LaunchCfg &cfg) {
+  CellArgs a = in;
+  a.lane_items = cfg.lane_items < 1 ? 1 : cfg.lane_items;
+  int spans = 0;
+  for (int l = 0; l < K; l = span_end_of(K, l)) ++spans;
+  // Carry-over pays for one span; with several spans it was measured slower
+  // (the heads left for a warp's next chunk, far away in index order, write
+  // their narrow-panel sectors long after their neighbours').
+  const bool carry = cfg.compact_carry > 0 || (cfg.compact_carry == 0 && spans == 1);
+  a.compact = a.p <= cfg.compact_max_p ? (carry ? 2 : 1) : 0;
+  if (a.compact == 1) {
+    int most = cfg.compact_items > 0 ? cfg.compact_items : (spans > 1 ? 2 : 4);
+    if (most > FDP_REC_MAX_ITEMS) most = FDP_REC_MAX_ITEMS;
+    if (a.lane_items > most) a.lane_items = most;
+  } else if (a.compact == 2) {
+    // The carry-over store does not grow with the chunk: compact_items sets
+    // the chunk over which the prefix decode is shared.
+    a.lane_items = cfg.compact_items > 0 ? cfg.compact_items : kCarryItems;
+  }
+  return a;
+}
+
+static cudaError_t launch_cell_k(const DevTables &t, int K, const CellArgs &in, const LaunchCfg &cfg,
+                                 cudaStream_t s) {
+  const CellArgs a = schedule_cell(in, K, cfg);
   if (t.u64) {
 #define CALL64(k) launch_cell_t<uint64_t, k>(a, cfg, s)
     FDP_SWITCH_K(K, CALL64)
@@ -86,16 +113,7 @@ cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_
   a.cap = t.cap;
   a.blk_in_zero = blk_in_zero ? 1 : 0;
   a.blk_out_p1 = blk_out_p1 ? 1 : 0;
-  a.lane_items = cfg.lane_items < 1 ? 1 : cfg.lane_items;
   a.share_prefix = (t.W - 1 - p) >= cfg.share_min ? 1 : 0;
-  a.compact = p <= cfg.compact_max_p ? 1 : 0;
-  if (a.compact) {
-    int spans = 0;
-    for (int l = 0; l < K; l = span_end_of(K, l)) ++spans;
-    int most = cfg.compact_items > 0 ? cfg.compact_items : (spans > 1 ? 2 : 4);
-    if (most > FDP_REC_MAX_ITEMS) most = FDP_REC_MAX_ITEMS;
-    if (a.lane_items > most) a.lane_items = most;
-  }
   const bool one_panel = (K == 1 || K == 2 || K == 4 || K == 8);
   if (K > 8 && p >= cfg.split_spans_min_p && !cfg.split_panels) {
     // Each span (panels of at most 8 lanes together) is laid out exactly as a

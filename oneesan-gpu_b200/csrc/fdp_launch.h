@@ -11,6 +11,7 @@
 namespace fdp {
 
 constexpr int kMaxLanes = 16;  // K = 1..16 residues interleaved per state
+constexpr int kCarryItems = 16;  // default states per lane of a grouped chunk with carry-over queues
 
 // Per-(width, height cap) device table blob.
 struct DevTables {
@@ -30,11 +31,14 @@ struct LaunchCfg {
   int lane_items = 8;        // items per lane of a warp chunk of the cell kernel
   int share_min = 4;         // share the chunk's prefix decode when it walks >= this many positions
   int compact_max_p = 7;     // cells p <= this update a chunk's items grouped by centre type (-1: never)
-  int compact_items = 0;     // states per lane of a compacted chunk (1..FDP_REC_MAX_ITEMS; 0: 4 for
-                             // one span, 2 when closure sources are staged, which leaves L1 room)
+  int compact_items = 0;     // states per lane of a compacted chunk (without carry-over 1..FDP_REC_MAX_ITEMS;
+                             // 0: 4 for one span, 2 when closure sources are staged, which leaves L1
+                             // room; with carry-over 1..16, 0: kCarryItems)
+  int compact_carry = 0;     // grouped cells queue heads across chunks so every update runs 32 items
+                             // (1 on, -1 off, 0 automatic: on when the lanes fit one span)
   int row_init = 0;          // strip rows filled directly by the row-k initialiser (0: automatic, -1: never)
   bool row_init_tensor = true;  // the initialiser's products on the tensor cores (else the CUDA cores)
-  int split_spans_min_p = 1000; // cells p >= this run each span of a several-span lane count as its own launch
+  int split_spans_min_p = 1;    // cells p >= this run each span of a several-span lane count as its own launch
 };
 
 template <typename Idx, int K>

@@ -57,7 +57,7 @@ class Tuning(ctypes.Structure):
                 ("bounded_prefix", ctypes.c_int), ("lane_items", ctypes.c_int), ("share_min", ctypes.c_int),
                 ("compact_max_p", ctypes.c_int), ("compact_items", ctypes.c_int),
                 ("row_init_rows", ctypes.c_int), ("row_init_product", ctypes.c_int),
-                ("split_spans_min_p", ctypes.c_int)]
+                ("split_spans_min_p", ctypes.c_int), ("compact_carry", ctypes.c_int)]
 
 
 class AutotuneResult(ctypes.Structure):
@@ -296,9 +296,10 @@ class Engine:
     def set_tuning(self, block: int = 256, grid: int = 0, split_panels: bool = False,
                    bounded_prefix: bool = True, lane_items: int = 0, share_min: int = 0,
                    compact_max_p: int = 0, compact_items: int = 0, row_init_rows: int = 0,
-                   row_init_product: int = 0, split_spans_min_p: int = 0) -> None:
+                   row_init_product: int = 0, split_spans_min_p: int = 0, compact_carry: int = 0) -> None:
         t = Tuning(block, grid, 1 if split_panels else 0, 1 if bounded_prefix else 0, lane_items, share_min,
-                   compact_max_p, compact_items, row_init_rows, row_init_product, split_spans_min_p)
+                   compact_max_p, compact_items, row_init_rows, row_init_product, split_spans_min_p,
+                   compact_carry)
         _check(lib().fdp_set_tuning(self._ctx, ctypes.byref(t)), "fdp_set_tuning")
 
     def get_tuning(self) -> dict:
@@ -308,7 +309,7 @@ class Engine:
                 "bounded_prefix": bool(t.bounded_prefix), "lane_items": t.lane_items, "share_min": t.share_min,
                 "compact_max_p": t.compact_max_p, "compact_items": t.compact_items,
                 "row_init_rows": t.row_init_rows, "row_init_product": t.row_init_product,
-                "split_spans_min_p": t.split_spans_min_p}
+                "split_spans_min_p": t.split_spans_min_p, "compact_carry": t.compact_carry}
 
     # ---- serving -------------------------------------------------------------
     def server_start(self, hbm_budget_bytes: int, max_active: int = 8, max_lanes: int = 16,

@@ -96,19 +96,26 @@ def test_zero_input_stays_zero(engine):
 
 def test_tuning_never_changes_results(engine):
     # block size, grid size, panel splitting, warp-chunk size, prefix
-    # sharing, grouping and span splitting are performance knobs only
+    # sharing, grouping (per chunk or with carry-over queues) and span
+    # splitting are performance knobs only
     try:
-        for block, grid, split, items, share, compact, citems, spans in (
-                (128, 0, True, 1, 99, -1, 4, 1), (64, 37, False, 7, 1, 30, 3, 1000), (256, 1, True, 64, 1, 5, 1, 4),
-                (96, 0, False, 3, 5, 1, 2, 1), (256, 0, False, 1, 1, 30, 4, 6), (160, 3, False, 4, 2, 30, 4, 9)):
+        for block, grid, split, items, share, compact, citems, spans, carry in (
+                (128, 0, True, 1, 99, -1, 4, 1, -1), (64, 37, False, 7, 1, 30, 3, 1000, -1),
+                (256, 1, True, 64, 1, 5, 1, 4, 1), (96, 0, False, 3, 5, 1, 2, 1, -1),
+                (256, 0, False, 1, 1, 30, 4, 6, 1), (160, 3, False, 4, 2, 30, 4, 9, -1),
+                (256, 0, False, 8, 4, 30, 16, 1000, 1), (64, 5, False, 2, 2, 30, 8, 1000, 1),
+                (224, 0, True, 5, 3, 30, 1, 1000, 1)):
             engine.set_tuning(block=block, grid=grid, split_panels=split, lane_items=items, share_min=share,
-                              compact_max_p=compact, compact_items=citems, split_spans_min_p=spans)
+                              compact_max_p=compact, compact_items=citems, split_spans_min_p=spans,
+                              compact_carry=carry)
             assert engine.get_tuning() == {"block": block, "grid": grid, "split_panels": split,
                                            "bounded_prefix": True, "lane_items": items, "share_min": share,
                                            "compact_max_p": compact, "compact_items": citems,
-                                           "row_init_rows": 0, "row_init_product": 0, "split_spans_min_p": spans}
+                                           "row_init_rows": 0, "row_init_product": 0, "split_spans_min_p": spans,
+                                           "compact_carry": carry}
             _run(engine, 12, 11, 1, [MODS[i % 3] for i in range(14)], seed=block + grid)
             _run(engine, 12, 3, 1, [MODS[i % 3] for i in range(8)], seed=block + items)
+            _run(engine, 12, 5, 1, [MODS[i % 3] for i in range(5)], seed=block + citems)
     finally:
         engine.set_tuning()
 

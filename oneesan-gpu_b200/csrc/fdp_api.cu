@@ -303,16 +303,14 @@ fdp_status fdp_enqueue_pass(fdp_ctx *c, const DevTables &t, int L, const uint32_
     if ((st = space(caps[size_t(row - 1)], &cur)) != FDP_OK) return st;
     if (cur != prev) FDP_CK(fdp::enqueue_expand(*prev, *cur, L, main, blk, D * uint64_t(L), s, &n), "grow state");
     for (int p = W - 1; p >= 1; --p) {
-      FDP_CK(fdp::launch_cell(*cur, L, mods, main, blk, p, p == W - 1, false, c->cfg, s), "bounded cell");
-      ++n;
+      FDP_CK(fdp::launch_cell(*cur, L, mods, main, blk, p, p == W - 1, false, c->cfg, s, &n), "bounded cell");
     }
     prev = cur;
   }
   if (prev != &t) FDP_CK(fdp::enqueue_expand(*prev, t, L, main, blk, D * uint64_t(L), s, &n), "grow state");
   for (int row = next_row > B + 1 ? next_row : B + 1; row <= fdp::sweep_rows(W); ++row)
     for (int p = W - 1; p >= 1; --p) {
-      FDP_CK(fdp::launch_cell(t, L, mods, main, blk, p, p == W - 1, false, c->cfg, s), "cell");
-      ++n;
+      FDP_CK(fdp::launch_cell(t, L, mods, main, blk, p, p == W - 1, false, c->cfg, s, &n), "cell");
     }
   FDP_CK(fdp::launch_first_row_dot(t, L, mods, main, acc, d_res, s), "first-row dot");
   n += 2;

@@ -99,7 +99,7 @@ static cudaError_t launch_cell_k(const DevTables &t, int K, const CellArgs &in, 
 }
 
 cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_t *main, uint32_t *blk, int p,
-                        bool blk_in_zero, bool blk_out_p1, const LaunchCfg &cfg, cudaStream_t s) {
+                        bool blk_in_zero, bool blk_out_p1, const LaunchCfg &cfg, cudaStream_t s, uint64_t *kernels) {
   if (!t.ptr || p < 1 || p >= t.W || K < 1 || K > kMaxLanes) return cudaErrorInvalidValue;
   CellArgs a{};
   a.tables = t.ptr;
@@ -128,11 +128,15 @@ cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_
       for (int i = 0; i < le - l0; ++i) b.mod[i] = mods[l0 + i];
       cudaError_t e = launch_cell_k(t, le - l0, b, cfg, s);
       if (e != cudaSuccess) return e;
+      if (kernels) ++*kernels;
       l0 = le;
     }
     return cudaSuccess;
   }
-  if (one_panel || !cfg.split_panels) return launch_cell_k(t, K, a, cfg, s);
+  if (one_panel || !cfg.split_panels) {
+    if (kernels) ++*kernels;
+    return launch_cell_k(t, K, a, cfg, s);
+  }
   // Every panel is an independent [N][PW] array: run each as its own K = PW problem.
   for (int l0 = 0; l0 < K;) {
     const int pw = (K - l0 >= 8) ? 8 : (K - l0 >= 4) ? 4 : (K - l0 >= 2) ? 2 : 1;
@@ -142,6 +146,7 @@ cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_
     for (int i = 0; i < pw; ++i) b.mod[i] = mods[l0 + i];
     cudaError_t e = launch_cell_k(t, pw, b, cfg, s);
     if (e != cudaSuccess) return e;
+    if (kernels) ++*kernels;
     l0 += pw;
   }
   return cudaSuccess;

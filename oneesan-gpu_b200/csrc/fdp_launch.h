@@ -46,9 +46,12 @@ cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t 
 template <typename Idx, int K>
 cudaError_t launch_first_row_t(const FirstRowArgs &a, bool dot, cudaStream_t s);
 
-// One cell p on [M][K] / [D][K] arrays.
+// One cell p on [M][K] / [D][K] arrays: one kernel launch, or one per lane
+// span or panel when the configuration splits them; *kernels (if given) is
+// increased by the launches made.
 cudaError_t launch_cell(const DevTables &t, int K, const uint32_t *mods, uint32_t *main, uint32_t *blk, int p,
-                        bool blk_in_zero, bool blk_out_p1, const LaunchCfg &cfg, cudaStream_t s);
+                        bool blk_in_zero, bool blk_out_p1, const LaunchCfg &cfg, cudaStream_t s,
+                        uint64_t *kernels = nullptr);
 // main[rank(first-row state)] = 1 for every first-row mask.
 cudaError_t launch_first_row_init(const DevTables &t, int K, uint32_t *main, cudaStream_t s);
 // acc[k] += sum over first-row states of main[.][k]; then residues[k] = acc[k] mod p_k.

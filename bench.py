@@ -11,9 +11,10 @@ value    residues/hour from the device time of the captured pass (CUDA events
          on the engine's stream), max over ranks.
 e2e      residues/hour through the public C ABI call fdp_run_sync from host
          buffers (moduli in, residues out) including graph capture.
-roofline the per-cell transition kernel: algorithmic bytes per launch
+roofline the per-cell transition kernel: algorithmic bytes per cell
          (fdp_cell_bytes: 4 x words that must be read + 4 x words that can
-         change, per modulus) over its CUDA-event duration.
+         change, per modulus) over the cell's CUDA-event duration (with 14
+         lanes a cell is two launches, one per lane span of at most 8).
 
 --impl reference times the reference's own CPU counter (third_party/ggcount,
 built unmodified into oracle/_ref) on all host threads: each step is one
@@ -108,11 +109,12 @@ def published_check(n: int, moduli, residues) -> dict:
 
 
 def committed_traffic(n: int, lanes: int):
-    """Per-launch DRAM bytes of the cell kernel from the committed ncu summary."""
+    """DRAM bytes per cell (all of the cell's lane-span launches) of the cell
+    kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "cell_kernel_traffic.txt")
     if not os.path.exists(path):
         return None
-    pat = re.compile(rf"^n={n}\s+lanes={lanes}\s+dram_bytes_per_launch=(\d+)")
+    pat = re.compile(rf"^n={n}\s+lanes={lanes}\s+dram_bytes_per_cell=(\d+)")
     with open(path) as f:
         for line in f:
             m = pat.match(line.strip())
@@ -382,8 +384,12 @@ def run_ours(args) -> None:
         extra["plain"] = {"value": 3600.0 / rp.stats.device_s, "unit": "residues/hour",
                           "sample": "one residue, lanes=1", "device_s": rp.stats.device_s}
 
-    # Roofline of the dominant kernel: per-cell CUDA-event times of one row sweep.
+    # Roofline of the dominant kernel: per-cell CUDA-event times of one row sweep
+    # (a cell of more than 8 lanes is one launch per lane span of at most 8).
     cell_ms = eng.time_cells(n, moduli, lanes, rows=args.profile_rows)
+    tuning = eng.get_tuning()
+    split = lanes > 8 and not tuning["split_panels"] and tuning["split_spans_min_p"] <= 1
+    launches_per_cell = len(fdp.lane_spans(lanes)) if split else 1
     tot_bytes = sum(fdp.cell_bytes(W, p) * lanes for p in range(1, W))
     tot_ms = sum(cell_ms[1:])
     achieved = tot_bytes / (tot_ms * 1e-3) / 1e9
@@ -392,10 +398,9 @@ def run_ours(args) -> None:
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
             "kernel": "cell_kernel (per-cell frontier transition)", "peak_source": peaks["source"],
-            "alg_bytes_per_launch": tot_bytes / (W - 1), "mean_launch_ms": tot_ms / (W - 1),
-            "row_ms": tot_ms,
+            "alg_bytes_per_cell": tot_bytes / (W - 1), "mean_cell_ms": tot_ms / (W - 1),
+            "launches_per_cell": launches_per_cell, "row_ms": tot_ms,
             "cell_gbs": [fdp.cell_bytes(W, p) * lanes / (cell_ms[p] * 1e-3) / 1e9 for p in range(1, W)]}
-    tuning = eng.get_tuning()
     eng.close()  # frees the state before the sub-runs below
 
     transitions = plan.transitions_per_residue * k * args.steps * world

@@ -170,6 +170,21 @@ def lane_panels(lanes: int) -> list:
     return out
 
 
+def lane_spans(lanes: int) -> list:
+    """Spans (first lane, end lane) of consecutive panels holding at most 8
+    lanes together; a cell of several spans may run as one launch per span."""
+    out, l0 = [], 0
+    panels = lane_panels(lanes)
+    i = 0
+    while i < len(panels):
+        start, width = panels[i][0], 0
+        while i < len(panels) and width + panels[i][1] <= 8:
+            width += panels[i][1]
+            i += 1
+        out.append((start, start + width))
+    return out
+
+
 def pack_lanes(a):
     """(N, lanes) uint32 array -> flat array in the engine's panel layout."""
     import numpy as np

@@ -92,6 +92,7 @@ PUBLISHED = {
     (20, 4294967291): 2308006916,  # scripts/test/groupbatch-scratch.py:17
     (20, 4294966997): 3704549185,
     (18, 4294967291): 503411004,   # docs/results/reverse-algorithm-2026-09-05.md:53
+    (23, 4294967291): 2762394459,  # docs/b300-hbm32.md:382-385
 }
 
 
@@ -424,6 +425,8 @@ def run_ours(args) -> None:
     line.update(extra)
     if rank == 0 and world == 1 and not args.no_n20:
         line["n20"] = run_n20(local)
+    if rank == 0 and world == 1 and not args.no_n23:
+        line["n23"] = run_n23(local)
     if rank == 0 and world == 1 and not args.no_serve:
         line["serving"] = run_serving_stream(args.seed, args.serve_requests, args.serve_gap, 0.1,
                                              args.serve_budget_gb, args.serve_slots)
@@ -456,6 +459,31 @@ def run_n20(device: int) -> dict:
     out["checked_against"] = "reference CPU counter (ggcount), tests/golden/ggcount_residues.json"
     out["batched_over_plain"] = out["batched"]["residues_per_hour"] / out["plain"]["residues_per_hour"]
     return out
+
+
+def run_n23(device: int, budget: int = 170 * 10**9) -> dict:
+    """Config 5: n = 23 at HBM capacity.  The largest number of the largest
+    primes below 2^32 whose state and tables fit the budget runs as one pass;
+    its residue mod 4294967291 is checked against the published value."""
+    import fdp
+    lanes = 0
+    for cand in range(fdp.MAX_LANES, 0, -1):
+        pl = fdp.plan(23, primes_below_2_32(cand), cand, budget)
+        if pl.fits and pl.passes == 1:
+            lanes = cand
+            break
+    if not lanes:
+        return {"skipped": "no lane count of n = 23 fits the budget"}
+    mods = primes_below_2_32(lanes)
+    pl = fdp.plan(23, mods, lanes, budget)
+    with fdp.Engine(device) as eng:
+        r = eng.residues(23, mods, lanes)
+    if r.residues[0] != PUBLISHED[(23, 4294967291)]:
+        raise SystemExit(f"n=23 mod 4294967291: residue {r.residues[0]} != published {PUBLISHED[(23, 4294967291)]}")
+    return {"lanes": lanes, "budget_gb": budget / 1e9, "state_gib": pl.state_bytes / 2**30,
+            "device_s": r.stats.device_s, "residues_per_hour": 3600.0 * lanes / r.stats.device_s,
+            "residues": r.residues, "checked": {"modulus": 4294967291, "residue": r.residues[0],
+                                                "published": "docs/b300-hbm32.md:382-385 of the reference"}}
 
 
 def run_serving_stream(seed: int, count: int, gap: float, time_scale: float, budget_gb: float,
@@ -567,6 +595,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-n20", action="store_true", help="skip the n=20 plain/batched sub-record")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream sub-record")
+    ap.add_argument("--no-n23", action="store_true", help="skip the n=23 at-capacity sub-record")
     ap.add_argument("--serve", action="store_true", help="run the serving stream instead")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--serve-requests", type=int, default=200)

@@ -398,7 +398,8 @@ def run_ours(args) -> None:
     traffic = committed_traffic(n, lanes)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-            "kernel": "cell_kernel (per-cell frontier transition)", "peak_source": peaks["source"],
+            "kernel": "cell_kernel / cell_stream_kernel (per-cell frontier transition)",
+            "peak_source": peaks["source"],
             "alg_bytes_per_cell": tot_bytes / (W - 1), "mean_cell_ms": tot_ms / (W - 1),
             "launches_per_cell": launches_per_cell, "row_ms": tot_ms,
             "cell_gbs": [fdp.cell_bytes(W, p) * lanes / (cell_ms[p] * 1e-3) / 1e9 for p in range(1, W)]}

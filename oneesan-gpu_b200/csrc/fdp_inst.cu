@@ -49,11 +49,14 @@ cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t 
       if (carry > most) most = carry;
       e = cudaFuncSetAttribute(cell_kernel<Idx, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(most));
       if (e != cudaSuccess) return e;
+      e = cudaFuncSetAttribute(cell_stream_kernel<Idx, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(most));
+      if (e != cudaSuccess) return e;
       v.limit_set = true;
     }
-    int &slot = v.per_sm[(uint64_t(cfg.block) << 32) | uint64_t(smem)];
+    int &slot = v.per_sm[(uint64_t(a.compact ? 1 : 0) << 62) | (uint64_t(cfg.block) << 32) | uint64_t(smem)];
     if (slot == 0) {
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&slot, cell_kernel<Idx, K>, cfg.block, smem);
+      e = a.compact ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&slot, cell_kernel<Idx, K>, cfg.block, smem)
+                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&slot, cell_stream_kernel<Idx, K>, cfg.block, smem);
       if (e != cudaSuccess) {
         slot = 0;
         return e;
@@ -66,7 +69,8 @@ cudaError_t launch_cell_t(const CellArgs &a, const LaunchCfg &cfg, cudaStream_t 
   const uint64_t per_block = uint64_t(cfg.block) * uint64_t(a.lane_items < 1 ? 1 : a.lane_items);
   const uint64_t need = (a.items + per_block - 1) / per_block;
   if (uint64_t(grid) > need) grid = int(need ? need : 1);
-  cell_kernel<Idx, K><<<grid, cfg.block, smem, s>>>(a);
+  if (a.compact) cell_kernel<Idx, K><<<grid, cfg.block, smem, s>>>(a);
+  else cell_stream_kernel<Idx, K><<<grid, cfg.block, smem, s>>>(a);
   return cudaGetLastError();
 }
 

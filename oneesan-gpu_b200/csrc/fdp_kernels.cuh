@@ -45,14 +45,14 @@ FDP_HD constexpr size_t cell_smem_bytes(int block, int W, int compact, int rec_i
   return cell_recs_offset<Idx, K>(block, W) + size_t(block / 32) * cell_recs_per_warp<Idx>(compact, rec_items);
 }
 
-// Resident CTAs of 256 threads per SM the cell kernel is compiled for (the
-// register budget per thread is 65536 / (256 x this)).
+// Resident CTAs of 256 threads per SM the cell kernels of six or more lanes
+// are compiled for (64 registers per thread).
 #ifndef FDP_CELL_MIN_BLOCKS
 #define FDP_CELL_MIN_BLOCKS 4
 #endif
 
-template <typename Idx, int K>
-__global__ void __launch_bounds__(256, FDP_CELL_MIN_BLOCKS) cell_kernel(const CellArgs a) {
+template <typename Idx, int K, bool GROUPED>
+__device__ __forceinline__ void cell_body(const CellArgs &a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CellSmem<Idx> &sm = *reinterpret_cast<CellSmem<Idx> *>(smem_raw);
   Idx *cand = reinterpret_cast<Idx *>(smem_raw + sizeof(CellSmem<Idx>));
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(256, FDP_CELL_MIN_BLOCKS) cell_kernel(const Ce
   // the front and c = N from the back, so each update runs on whole warps
   // instead of two half-empty branches.  Any order of items within a cell is
   // valid: no item reads or writes a word another item writes.
-  const int compact = a.compact == 2 ? 2 : (a.compact && a.lane_items <= FDP_REC_MAX_ITEMS ? 1 : 0);
+  const int compact = !GROUPED ? 0 : (a.compact == 2 ? 2 : (a.compact && a.lane_items <= FDP_REC_MAX_ITEMS ? 1 : 0));
   unsigned char *const recs = smem_raw + cell_recs_offset<Idx, K>(blockDim.x, a.W) +
                               size_t(threadIdx.x >> 5) * cell_recs_per_warp<Idx>(compact, a.lane_items);
   const HeadRecs<Idx> rec{recs, int(chunk)};
@@ -143,6 +143,30 @@ __global__ void __launch_bounds__(256, FDP_CELL_MIN_BLOCKS) cell_kernel(const Ce
   // Whatever the carry-over queues still hold.
   if (int(lane) < qx) apply_x<Idx, K>(a, cr.f(0)[lane], cr.f(1)[lane], cr.f(2)[lane]);
   if (int(lane) < qn) item_n<Idx, K>(a, sm, cr.get_n(int(lane)), cand + threadIdx.x, int(blockDim.x));
+}
+
+// Resident CTAs of 256 threads per SM each variant is compiled for (the
+// register budget per thread is 65536 / (256 x this)): narrow lane counts need
+// fewer registers per item, so more warps keep loads in flight.  Measured at
+// n = 22: one lane large-p cells 136 -> 109 ms per row at 6 CTAs (40
+// registers); 2-4 lanes gain 3 % on their grouped cells at 5; six or more
+// lanes are slower at 5 or 6 (spills), and stay at 4.
+template <int K>
+constexpr int group_min_blocks() { return (K >= 2 && K <= 4) ? 5 : FDP_CELL_MIN_BLOCKS; }
+template <int K>
+constexpr int stream_min_blocks() { return K <= 4 ? 6 : FDP_CELL_MIN_BLOCKS; }
+
+// The cell kernel of the cells whose items are grouped by centre type (small
+// p) and the one of the cells that stream them in index order (the rest):
+// the same body, compiled apart so that each gets its own register budget.
+template <typename Idx, int K>
+__global__ void __launch_bounds__(256, group_min_blocks<K>()) cell_kernel(const CellArgs a) {
+  cell_body<Idx, K, true>(a);
+}
+
+template <typename Idx, int K>
+__global__ void __launch_bounds__(256, stream_min_blocks<K>()) cell_stream_kernel(const CellArgs a) {
+  cell_body<Idx, K, false>(a);
 }
 
 template <typename Idx, int K>

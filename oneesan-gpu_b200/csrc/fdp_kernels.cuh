@@ -45,8 +45,8 @@ FDP_HD constexpr size_t cell_smem_bytes(int block, int W, int compact, int rec_i
   return cell_recs_offset<Idx, K>(block, W) + size_t(block / 32) * cell_recs_per_warp<Idx>(compact, rec_items);
 }
 
-// Resident CTAs of 256 threads per SM the cell kernels of six or more lanes
-// are compiled for (64 registers per thread).
+// Resident CTAs of 256 threads per SM the cell kernels are compiled for
+// unless a lane count has its own budget below (64 registers per thread).
 #ifndef FDP_CELL_MIN_BLOCKS
 #define FDP_CELL_MIN_BLOCKS 4
 #endif
@@ -148,9 +148,10 @@ __device__ __forceinline__ void cell_body(const CellArgs &a) {
 // Resident CTAs of 256 threads per SM each variant is compiled for (the
 // register budget per thread is 65536 / (256 x this)): narrow lane counts need
 // fewer registers per item, so more warps keep loads in flight.  Measured at
-// n = 22: one lane large-p cells 136 -> 109 ms per row at 6 CTAs (40
-// registers); 2-4 lanes gain 3 % on their grouped cells at 5; six or more
-// lanes are slower at 5 or 6 (spills), and stay at 4.
+// n = 22: the streaming cells of one lane 136 -> 109 ms per row at 6 CTAs (40
+// registers), 2 and 4 lanes gain there too; the grouped cells of 2-4 lanes
+// gain 3 % at 5 CTAs, those of one lane do not; 6 and 8 lanes spill and run
+// 2-7 % slower at 5 or 6, so lane counts above 4 stay at 4.
 template <int K>
 constexpr int group_min_blocks() { return (K >= 2 && K <= 4) ? 5 : FDP_CELL_MIN_BLOCKS; }
 template <int K>

@@ -7,7 +7,8 @@
 //            4294966997}; items visited in warp chunks of 32..256 with the
 //            shared prefix decode, in index order or in the grouped order of
 //            the small-p kernel path (every c = R/L item, then the c = N items
-//            backwards), exactly as the kernel may schedule them.
+//            backwards), exactly as the kernel may schedule them; the first
+//            cell of a row also with a blocked input known to be zero.
 //   capped : the same in the height-bounded spaces (caps 1..4): input supported
 //            on the capped space, full-space oracle operator, projection back.
 //   expand : the walk that moves a vector between spaces
@@ -62,7 +63,7 @@ static int run_cells(int W, int cap, uint64_t seed) {
     a.p = p;
     a.items = D;
     a.mstates = M;
-    a.blk_in_zero = 0;
+    a.blk_in_zero = (p == W - 1 && (seed & 2)) ? 1 : 0;
     a.blk_out_p1 = 1;
     a.cap = cap;
     for (int k = 0; k < K; ++k) a.mod[k] = mods[(k + p) % 3];
@@ -70,7 +71,7 @@ static int run_cells(int W, int cap, uint64_t seed) {
     for (uint64_t i = 0; i < M; ++i)
       for (int k = 0; k < K; ++k) mi[lane_word(K, M, i, k)] = uint32_t(rng() % a.mod[k]);
     for (uint64_t i = 0; i < D; ++i)
-      for (int k = 0; k < K; ++k) bi[lane_word(K, D, i, k)] = uint32_t(rng() % a.mod[k]);
+      for (int k = 0; k < K; ++k) bi[lane_word(K, D, i, k)] = a.blk_in_zero ? 0u : uint32_t(rng() % a.mod[k]);
     std::vector<uint32_t> gm = mi, gb = bi;
     a.main = gm.data();
     a.blk = gb.data();

@@ -83,3 +83,20 @@ def test_create_without_gpu_reports_gpu_count():
     with pytest.raises(fdp.FdpError) as e:
         fdp.Engine(0)
     assert e.value.status == fdp.FDP_ERR_GPU_COUNT
+
+
+def test_lane_panels_and_spans():
+    # Panels are greedy widths 8, 4, 2, 1; a span is consecutive panels holding
+    # at most 8 lanes (the unit a cell launch of several spans splits into).
+    import fdp
+    for lanes in range(1, 17):
+        panels = fdp.lane_panels(lanes)
+        assert sum(w for _, w in panels) == lanes
+        assert [w for _, w in panels] == sorted((w for _, w in panels), reverse=True)
+        spans = fdp.lane_spans(lanes)
+        assert spans[0][0] == 0 and spans[-1][1] == lanes
+        assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+        assert all(0 < e - s <= 8 for s, e in spans)
+        assert all(any(p == s for p, _ in panels) for s, _ in spans)  # spans start on a panel
+    assert fdp.lane_spans(14) == [(0, 8), (8, 14)]
+    assert fdp.lane_spans(8) == [(0, 8)] and fdp.lane_spans(6) == [(0, 6)]

@@ -68,9 +68,8 @@ static CellArgs schedule_cell(const CellArgs &in, int K, const LaunchCfg &cfg) {
   a.lane_items = cfg.lane_items < 1 ? 1 : cfg.lane_items;
   int spans = 0;
   for (int l = 0; l < K; l = span_end_of(K, l)) ++spans;
-  // Carry-over pays for one span; with several spans it was measured slower
-  // (the heads left for a warp's next chunk, far away in index order, write
-  // their narrow-panel sectors long after their neighbours').
+  // Carry-over pays for one span; in a launch of several spans (closure
+  // sources staged in shared memory) it was measured slower.
   const bool carry = cfg.compact_carry > 0 || (cfg.compact_carry == 0 && spans == 1);
   a.compact = a.p <= cfg.compact_max_p ? (carry ? 2 : 1) : 0;
   if (a.compact == 1) {

@@ -66,6 +66,12 @@ void free_tables(DevTables *t) {
 static CellArgs schedule_cell(const CellArgs &in, int K, const LaunchCfg &cfg) {
   CellArgs a = in;
   a.lane_items = cfg.lane_items < 1 ? 1 : cfg.lane_items;
+  // A small problem runs at most as many items per lane as fill every
+  // resident thread once: longer warp chunks would leave most SMs idle behind
+  // a few warps' serial chains (n = 10, one lane: 2.65 -> 0.78 ms per pass).
+  const uint64_t resident = uint64_t(device_sm_count()) * 4 * 256;  // 4 CTAs of 256 threads per SM
+  const uint64_t fill = a.items / resident > 1 ? a.items / resident : 1;
+  if (uint64_t(a.lane_items) > fill) a.lane_items = int(fill);
   int spans = 0;
   for (int l = 0; l < K; l = span_end_of(K, l)) ++spans;
   // Carry-over pays for one span; in a launch of several spans (closure
@@ -80,6 +86,7 @@ static CellArgs schedule_cell(const CellArgs &in, int K, const LaunchCfg &cfg) {
     // The carry-over store does not grow with the chunk: compact_items sets
     // the chunk over which the prefix decode is shared.
     a.lane_items = cfg.compact_items > 0 ? cfg.compact_items : kCarryItems;
+    if (uint64_t(a.lane_items) > fill) a.lane_items = int(fill);
   }
   return a;
 }

@@ -430,7 +430,7 @@ def run_ours(args) -> None:
         line["n23"] = run_n23(local)
     if rank == 0 and world == 1 and not args.no_serve:
         line["serving"] = run_serving_stream(args.seed, args.serve_requests, args.serve_gap, 0.1,
-                                             args.serve_budget_gb, args.serve_slots)
+                                             args.serve_budget_gb, args.serve_slots, args.serve_max_lanes)
     if rank == 0 and world == 1 and not args.no_cpu:
         s = ggcount_sample()
         line["cpu_baseline"] = cpu_baseline_record(s, n, scale_cpu(s, n))
@@ -488,7 +488,7 @@ def run_n23(device: int, budget: int = 170 * 10**9) -> dict:
 
 
 def run_serving_stream(seed: int, count: int, gap: float, time_scale: float, budget_gb: float,
-                       slots: int) -> dict:
+                       slots: int, max_lanes: int = 16) -> dict:
     """The serving stream: seeded Poisson arrivals, n ~ U{12..21}, k ~ U{1..8}
     largest-below-2^32 primes, admission under an HBM budget.  Every residue
     is checked against the same request run alone through fdp_run_sync."""
@@ -511,7 +511,7 @@ def run_serving_stream(seed: int, count: int, gap: float, time_scale: float, bud
         alone[n] = eng.residues(n, primes, 8).residues
     eng.close()
     eng = fdp.Engine(0)
-    eng.server_start(int(budget_gb * 1e9), max_active=slots, max_lanes=8)
+    eng.server_start(int(budget_gb * 1e9), max_active=slots, max_lanes=max_lanes)
     ids = [None] * len(reqs)
     t0 = time.perf_counter()
 
@@ -547,7 +547,7 @@ def run_serving_stream(seed: int, count: int, gap: float, time_scale: float, bud
     return {
         "workload": f"seed {seed}: {len(reqs)} requests, Poisson arrivals mean gap {gap} s x time scale "
                     f"{time_scale}, n~U{{12..21}}, k~U{{1..8}} largest primes below 2^32",
-        "budget_gb": budget_gb, "slots": slots, "max_lanes": 8,
+        "budget_gb": budget_gb, "slots": slots, "max_lanes": max_lanes,
         "p50_latency_s": pct(0.5), "p99_latency_s": pct(0.99), "max_latency_s": lat[-1],
         "mean_queue_s": statistics.mean(r["queue_s"] for r in results),
         "throughput_residues_per_hour": 3600.0 * residues / makespan,
@@ -560,11 +560,11 @@ def run_serving_stream(seed: int, count: int, gap: float, time_scale: float, bud
 
 def run_serving(args) -> None:
     rec = run_serving_stream(args.seed, args.serve_requests, args.serve_gap, args.serve_time_scale,
-                             args.serve_budget_gb, args.serve_slots)
+                             args.serve_budget_gb, args.serve_slots, args.serve_max_lanes)
     line = {"metric": "serving stream latency and throughput (continuous batching)",
             "value": rec["p50_latency_s"], "unit": "s (p50 latency)", "higher_is_better": False, "n_gpus": 1,
             "dtype": "u32", "config": {"workload": rec["workload"], "budget_gb": rec["budget_gb"],
-                                       "slots": rec["slots"], "max_lanes": 8}}
+                                       "slots": rec["slots"], "max_lanes": rec["max_lanes"]}}
     line.update(rec)
     print(json.dumps(line), flush=True)
 
@@ -604,6 +604,8 @@ def main() -> None:
     ap.add_argument("--serve-time-scale", type=float, default=1.0)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-max-lanes", type=int, default=16,
+                    help="residues per pass of a served request, shared by same-n requests that ride along")
     ap.add_argument("--cells-only", action="store_true",
                     help="profiling case: one row sweep of separately launched cells on a resident state")
     args = ap.parse_args()

@@ -231,13 +231,16 @@ fdp_status fdp_get_tuning(fdp_ctx *ctx, fdp_tuning *tuning);
  * it finishes).  Later, smaller requests may pass a request that does not fit
  * yet, unless it has waited longer than max_bypass_s.  Each admitted request
  * runs its residue pass(es) as one CUDA graph on its own stream, so admitted
- * requests overlap on the GPU and finish independently.  Results are exact and
- * the same as fdp_run_sync's for the same problem.
+ * requests overlap on the GPU and finish independently.  A request whose
+ * moduli fill less than one pass of max_lanes takes along later queued
+ * requests of the same n while their moduli fit, so one pass serves them all
+ * (fdp_request_info then reports the shared pass's lanes).  Results are exact
+ * and the same as fdp_run_sync's for the same problem.
  */
 typedef struct fdp_server_config {
   uint64_t hbm_budget_bytes;  /* device pool reserved for frontiers              */
   int max_active;             /* concurrent requests on the GPU (1..64)          */
-  int max_lanes;              /* residues per pass of one request (1..16)        */
+  int max_lanes;              /* residues per pass (1..16), shared by same-n riders */
   double max_bypass_s;        /* backfill limit; <= 0 means 30 s                  */
 } fdp_server_config;
 

@@ -9,7 +9,10 @@
 // whole computation (every pass of `lanes` residues: zero, row-0 init, row
 // sweeps, first-row dot, residue copy) as one CUDA graph and launches it on the
 // slot's own stream.  Requests on different slots therefore overlap on the
-// GPU.  Every wait is bounded: the scheduler sleeps at most 200 us between
+// GPU.  An admitted request whose moduli fill less than one pass takes along
+// later queued requests of the same n while their moduli fit its lanes, so
+// one pass serves them all (a residue does not depend on the other lanes).
+// Every wait is bounded: the scheduler sleeps at most 200 us between
 // event polls, and fdp_wait returns FDP_TIMEOUT after its limit.
 #include <algorithm>
 #include <chrono>
@@ -91,6 +94,10 @@ struct Job {
   Clock::time_point t_submit, t_admit, t_done;
   cudaGraphExec_t exec = nullptr;
   double device_s = 0;
+  // Queued requests of the same n whose moduli fit this request's one pass:
+  // they ride in its lanes (batch = its moduli, then each rider's).
+  std::vector<Job *> riders;
+  std::vector<uint32_t> batch;
 };
 
 // Bytes of one request in the pool: the state for `lanes` residues, then the
@@ -154,9 +161,10 @@ struct fdp_server {
     if (e != cudaSuccess) return fdp_cuda_status(e, "serve: begin capture");
     fdp_status es = fdp_cuda_status(fdp_enqueue_err_reset(derr, s), "serve: error word");
     uint64_t launches = 0;
-    for (int done = 0; done < int(j->mods.size()) && es == FDP_OK; done += j->lanes) {
-      const int L = std::min(j->lanes, int(j->mods.size()) - done);
-      es = fdp_enqueue_pass(ctx, *t, L, j->mods.data() + done, main, blk, acc, dres, pinned[size_t(slot)] + done,
+    const std::vector<uint32_t> &mods = j->batch.empty() ? j->mods : j->batch;
+    for (int done = 0; done < int(mods.size()) && es == FDP_OK; done += j->lanes) {
+      const int L = std::min(j->lanes, int(mods.size()) - done);
+      es = fdp_enqueue_pass(ctx, *t, L, mods.data() + done, main, blk, acc, dres, pinned[size_t(slot)] + done,
                             derr, s, &launches);
     }
     if (es == FDP_OK) es = fdp_cuda_status(fdp_enqueue_err_read(herr, derr, s), "serve: error word");
@@ -184,19 +192,26 @@ struct fdp_server {
     alloc.release(j->off, j->bytes);
     if (j->exec) cudaGraphExecDestroy(j->exec);
     j->exec = nullptr;
-    j->t_done = Clock::now();
     const unsigned int herr = pinned[size_t(slot)][kMaxModuliPerRequest];
-    if (ok && herr) {
-      fail(j, FDP_ERR_CUDA, "serve: a bounded wait on the device gave up; the residues are invalid");
-    } else if (ok) {
-      float ms = 0;
-      cudaEventElapsedTime(&ms, ev_start[size_t(slot)], ev_done[size_t(slot)]);
-      j->device_s = ms * 1e-3;
-      j->residues.assign(pinned[size_t(slot)], pinned[size_t(slot)] + j->mods.size());
-      j->state = Job::DONE;
-      ++completed;
-    } else {
-      fail(j, FDP_ERR_CUDA, std::string("serve: request failed: ") + cudaGetErrorString(err));
+    float ms = 0;
+    if (ok && !herr) cudaEventElapsedTime(&ms, ev_start[size_t(slot)], ev_done[size_t(slot)]);
+    const Clock::time_point now = Clock::now();
+    size_t at = 0;  // the leader's residues, then each rider's, in batch order
+    std::vector<Job *> all{j};
+    all.insert(all.end(), j->riders.begin(), j->riders.end());
+    for (Job *r : all) {
+      r->t_done = now;
+      if (ok && herr) {
+        fail(r, FDP_ERR_CUDA, "serve: a bounded wait on the device gave up; the residues are invalid");
+      } else if (ok) {
+        r->device_s = ms * 1e-3;
+        r->residues.assign(pinned[size_t(slot)] + at, pinned[size_t(slot)] + at + r->mods.size());
+        r->state = Job::DONE;
+        ++completed;
+      } else {
+        fail(r, FDP_ERR_CUDA, std::string("serve: request failed: ") + cudaGetErrorString(err));
+      }
+      at += r->mods.size();
     }
   }
 
@@ -228,18 +243,63 @@ struct fdp_server {
         for (int s = 0; s < int(slot_job.size()); ++s)
           if (!slot_job[size_t(s)]) { slot = s; break; }
         if (slot < 0) break;
+        std::vector<Job *> riders;
         for (auto it = queue.begin(); it != queue.end(); ++it) {
           Job *q = jobs[*it].get();
+          // Later queued requests of the same n ride in q's one pass while
+          // their moduli fit its lanes.
+          int total = int(q->mods.size());
+          if (total < cfg.max_lanes)
+            for (auto jt = std::next(it); jt != queue.end() && total < cfg.max_lanes; ++jt) {
+              Job *r = jobs[*jt].get();
+              if (r->n == q->n && total + int(r->mods.size()) <= cfg.max_lanes) {
+                riders.push_back(r);
+                total += int(r->mods.size());
+              }
+            }
           uint64_t off = 0;
-          if (alloc.alloc(q->bytes, &off)) {
+          uint64_t bytes = riders.empty() ? q->bytes : request_bytes(q->n, total);
+          bool got = alloc.alloc(bytes, &off);
+          if (!got && !riders.empty()) {  // the batch does not fit: the request alone
+            riders.clear();
+            total = int(q->mods.size());
+            bytes = q->bytes;
+            got = alloc.alloc(bytes, &off);
+          }
+          if (got) {
             q->off = off;
+            q->bytes = bytes;
+            if (!riders.empty()) {
+              q->lanes = total;
+              q->passes = 1;
+              q->batch = q->mods;
+              for (Job *r : riders) q->batch.insert(q->batch.end(), r->mods.begin(), r->mods.end());
+            }
             j = q;
             queue.erase(it);
             break;
           }
+          riders.clear();
           if (it == queue.begin() && secs(q->t_submit, now) > cfg.max_bypass_s) break;  // reserve for the head
         }
         if (!j) break;
+        if (!riders.empty()) {
+          std::deque<uint64_t> rest;
+          for (uint64_t id : queue) {
+            bool rides = false;
+            for (Job *r : riders) rides = rides || r->id == id;
+            if (!rides) rest.push_back(id);
+          }
+          queue.swap(rest);
+          for (Job *r : riders) {
+            r->slot = slot;
+            r->t_admit = now;
+            r->lanes = j->lanes;
+            r->passes = 1;
+            r->state = Job::LAUNCHING;
+          }
+          j->riders = riders;
+        }
         j->slot = slot;
         j->t_admit = now;
         j->state = Job::LAUNCHING;
@@ -257,8 +317,10 @@ struct fdp_server {
           if (j->exec) cudaGraphExecDestroy(j->exec);
           j->exec = nullptr;
           fail(j, st, "serve: launch failed: " + why);
+          for (Job *r : j->riders) fail(r, st, "serve: launch failed: " + why);
         } else {
           j->state = Job::RUNNING;
+          for (Job *r : j->riders) r->state = Job::RUNNING;
         }
       }
       cv.notify_all();  // wake fdp_wait callers

@@ -47,6 +47,26 @@ def test_results_in_the_mix_equal_results_alone(server_engine):
         assert res["passes"] == (len(mods) + 3) // 4 and res["latency_s"] >= res["run_s"]
 
 
+def test_same_n_requests_share_passes(server_engine):
+    # Requests of one n whose moduli fit one pass together ride in the same
+    # lanes: fewer passes than requests, and every result equal to it alone.
+    eng = server_engine
+    rng = random.Random(3)
+    reqs = [(13 if i % 2 else 14, rng.sample(P, rng.randint(1, 3))) for i in range(24)]
+    eng.server_start(hbm_budget_bytes=4 << 30, max_active=1, max_lanes=8)
+    try:
+        ids = [eng.submit(n, mods) for n, mods in reqs]
+        results = [eng.wait(rid, timeout_ms=120000) for rid in ids]
+        stats = eng.server_stats()
+    finally:
+        eng.server_stop()
+    assert stats["completed"] == 24 and stats["failed"] == 0
+    assert any(r["lanes"] > len(mods) for (_, mods), r in zip(reqs, results))  # some rode in another's lanes
+    assert all(r["lanes"] <= 8 and r["passes"] == 1 for r in results)
+    for (n, mods), res in zip(reqs, results):
+        assert res["residues"] == eng.residues(n, mods, lanes=len(mods)).residues, (n, mods)
+
+
 def test_budget_limits_admission(server_engine):
     eng = server_engine
     need = fdp.plan(17, P[:4], lanes=4).state_bytes

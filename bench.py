@@ -403,6 +403,13 @@ def run_ours(args) -> None:
             "alg_bytes_per_cell": tot_bytes / (W - 1), "mean_cell_ms": tot_ms / (W - 1),
             "launches_per_cell": launches_per_cell, "row_ms": tot_ms,
             "cell_gbs": [fdp.cell_bytes(W, p) * lanes / (cell_ms[p] * 1e-3) / 1e9 for p in range(1, W)]}
+    # The same bytes over the timed passes' device time: in a pass the two lane
+    # spans sweep as concurrent launch chains, which the per-cell timing (one
+    # span launch after the other) does not see; the row-k fill and the
+    # read-out are inside this time and not in the bytes.
+    pass_gbs = plan.alg_bytes_per_residue * k * args.steps / dev_s / 1e9
+    roof["pass_gbs"] = pass_gbs
+    roof["pass_frac"] = pass_gbs / peaks["hbm_gbs"]
     eng.close()  # frees the state before the sub-runs below
 
     transitions = plan.transitions_per_residue * k * args.steps * world

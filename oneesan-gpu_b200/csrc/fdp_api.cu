@@ -135,6 +135,9 @@ extern "C" fdp_status fdp_create(fdp_ctx **out, int device) {
   if (s == FDP_OK) s = cuda_status(cudaMallocHost(&c->h_err, sizeof(unsigned int)), "pinned error word");
   if (s == FDP_OK) s = cuda_status(cudaEventCreate(&c->ev0), "event");
   if (s == FDP_OK) s = cuda_status(cudaEventCreate(&c->ev1), "event");
+  if (s == FDP_OK) s = cuda_status(cudaStreamCreateWithFlags(&c->span_stream, cudaStreamNonBlocking), "span stream");
+  if (s == FDP_OK) s = cuda_status(cudaEventCreateWithFlags(&c->span_fork, cudaEventDisableTiming), "span event");
+  if (s == FDP_OK) s = cuda_status(cudaEventCreateWithFlags(&c->span_join, cudaEventDisableTiming), "span event");
   if (s != FDP_OK) {
     fdp_destroy(c);
     return s;
@@ -157,6 +160,9 @@ fdp_ctx::~fdp_ctx() {
   if (h_err) cudaFreeHost(h_err);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  if (span_fork) cudaEventDestroy(span_fork);
+  if (span_join) cudaEventDestroy(span_join);
+  if (span_stream) cudaStreamDestroy(span_stream);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -260,7 +266,8 @@ extern "C" fdp_status fdp_test_inject_pass_errors(int count) {
 
 fdp_status fdp_enqueue_pass(fdp_ctx *c, const DevTables &t, int L, const uint32_t *mods, uint32_t *main,
                             uint32_t *blk, unsigned long long *acc, uint32_t *d_res, uint32_t *h_res,
-                            unsigned int *d_err, cudaStream_t s, uint64_t *launches) {
+                            unsigned int *d_err, cudaStream_t s, uint64_t *launches, cudaStream_t span_stream,
+                            cudaEvent_t fork, cudaEvent_t join) {
   const int W = t.W;
   const uint64_t M = fdp::main_states(W), D = fdp::blocked_states(W);
   uint64_t n = 0;
@@ -308,10 +315,33 @@ fdp_status fdp_enqueue_pass(fdp_ctx *c, const DevTables &t, int L, const uint32_
     prev = cur;
   }
   if (prev != &t) FDP_CK(fdp::enqueue_expand(*prev, t, L, main, blk, D * uint64_t(L), s, &n), "grow state");
-  for (int row = next_row > B + 1 ? next_row : B + 1; row <= fdp::sweep_rows(W); ++row)
-    for (int p = W - 1; p >= 1; --p) {
-      FDP_CK(fdp::launch_cell(t, L, mods, main, blk, p, p == W - 1, false, c->cfg, s, &n), "cell");
+  const int row0 = next_row > B + 1 ? next_row : B + 1;
+  const bool chains = span_stream && fork && join && c->cfg.span_chains && L > 8 && !c->cfg.split_panels &&
+                      c->cfg.split_spans_min_p <= 1 && row0 <= fdp::sweep_rows(W);
+  if (chains) {
+    // Each lane span is laid out as a lane count of its own at its first
+    // panel's offset and no cell reads another span's panels, so the spans'
+    // row sweeps run as two chains of launches, joined before the read-out.
+    FDP_CK(cudaEventRecord(fork, s), "span fork");
+    FDP_CK(cudaStreamWaitEvent(span_stream, fork, 0), "span fork");
+    for (int l0 = 0, i = 0; l0 < L; ++i) {
+      const int le = fdp::span_end_of(L, l0);
+      cudaStream_t ss = i == 0 ? s : span_stream;
+      for (int row = row0; row <= fdp::sweep_rows(W); ++row)
+        for (int p = W - 1; p >= 1; --p)
+          FDP_CK(fdp::launch_cell(t, le - l0, mods + l0, main + size_t(l0) * M, blk + size_t(l0) * D, p, p == W - 1,
+                                  false, c->cfg, ss, &n),
+                 "cell");
+      l0 = le;
     }
+    FDP_CK(cudaEventRecord(join, span_stream), "span join");
+    FDP_CK(cudaStreamWaitEvent(s, join, 0), "span join");
+  } else {
+    for (int row = row0; row <= fdp::sweep_rows(W); ++row)
+      for (int p = W - 1; p >= 1; --p) {
+        FDP_CK(fdp::launch_cell(t, L, mods, main, blk, p, p == W - 1, false, c->cfg, s, &n), "cell");
+      }
+  }
   FDP_CK(fdp::launch_first_row_dot(t, L, mods, main, acc, d_res, s), "first-row dot");
   n += 2;
   if (h_res) FDP_CK(cudaMemcpyAsync(h_res, d_res, sizeof(uint32_t) * L, cudaMemcpyDeviceToHost, s), "residue copy");
@@ -348,7 +378,7 @@ extern "C" fdp_status fdp_run_sync(fdp_ctx *c, const fdp_problem *pr, uint32_t *
   for (int done = 0; done < pr->k && es == FDP_OK; done += lanes) {
     const int L = (pr->k - done) < lanes ? (pr->k - done) : lanes;
     es = fdp_enqueue_pass(c, *t, L, pr->moduli + done, c->d_main, c->d_blk, c->d_acc, c->d_res, c->h_res + done,
-                          c->d_err, c->stream, &launches);
+                          c->d_err, c->stream, &launches, c->span_stream, c->span_fork, c->span_join);
   }
   if (es == FDP_OK) es = cuda_status(fdp_enqueue_err_read(c->h_err, c->d_err, c->stream), "error word");
   cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
@@ -549,6 +579,8 @@ struct MultiPart {
   unsigned int *err = nullptr;  // this problem's error word
   cudaStream_t s = nullptr;
   cudaEvent_t done = nullptr;
+  cudaStream_t span_s = nullptr;  // the second lane span's sweep
+  cudaEvent_t span_fork = nullptr, span_join = nullptr;
 };
 
 extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, int count, uint32_t *residues_out,
@@ -582,6 +614,9 @@ extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, i
       if (p.err) cudaFree(p.err);
       if (p.s) cudaStreamDestroy(p.s);
       if (p.done) cudaEventDestroy(p.done);
+      if (p.span_s) cudaStreamDestroy(p.span_s);
+      if (p.span_fork) cudaEventDestroy(p.span_fork);
+      if (p.span_join) cudaEventDestroy(p.span_join);
     }
     if (pinned) cudaFreeHost(pinned);
     if (fork) cudaEventDestroy(fork);
@@ -606,6 +641,11 @@ extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, i
     MULTI_CK(cudaMalloc(&p.err, sizeof(unsigned int)), "multi error word");
     MULTI_CK(cudaStreamCreateWithFlags(&p.s, cudaStreamNonBlocking), "multi stream");
     MULTI_CK(cudaEventCreateWithFlags(&p.done, cudaEventDisableTiming), "multi event");
+    if (p.lanes > 8) {
+      MULTI_CK(cudaStreamCreateWithFlags(&p.span_s, cudaStreamNonBlocking), "multi stream");
+      MULTI_CK(cudaEventCreateWithFlags(&p.span_fork, cudaEventDisableTiming), "multi event");
+      MULTI_CK(cudaEventCreateWithFlags(&p.span_join, cudaEventDisableTiming), "multi event");
+    }
   }
   auto c0 = std::chrono::steady_clock::now();
   MULTI_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -618,7 +658,7 @@ extern "C" fdp_status fdp_run_multi_sync(fdp_ctx *c, const fdp_problem *probs, i
     for (int done = 0; done < probs[i].k && rs == FDP_OK; done += p.lanes) {
       const int L = (probs[i].k - done) < p.lanes ? (probs[i].k - done) : p.lanes;
       rs = fdp_enqueue_pass(c, *p.t, L, probs[i].moduli + done, p.main, p.blk, p.acc, p.res, pinned + off + done,
-                            p.err, p.s, &launches);
+                            p.err, p.s, &launches, p.span_s, p.span_fork, p.span_join);
     }
     if (rs == FDP_OK)
       rs = cuda_status(fdp_enqueue_err_read(reinterpret_cast<unsigned int *>(pinned + total_k + i), p.err, p.s),

@@ -21,6 +21,10 @@ struct fdp_ctx {
   unsigned int *d_err = nullptr;         // run_sync pass error word (device)
   unsigned int *h_err = nullptr;         // its copy after the pass (pinned host)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // A second stream for the sweep of the second lane span (lanes 8..): the
+  // spans touch disjoint panels, so their cell launches run as two chains.
+  cudaStream_t span_stream = nullptr;
+  cudaEvent_t span_fork = nullptr, span_join = nullptr;
   fdp::LaunchCfg cfg;
   std::mutex mu;         // serialises run_sync / apply_cells / time_cells / tuning
   std::mutex tables_mu;  // guards `tables` (also used by the serving thread)
@@ -31,9 +35,14 @@ struct fdp_ctx {
 fdp_status fdp_ctx_tables(fdp_ctx *c, int W, const fdp::DevTables **out);
 fdp_status fdp_ctx_tables_cap(fdp_ctx *c, int W, int cap, const fdp::DevTables **out);
 fdp_status fdp_prepare_pass(fdp_ctx *c, int W, const fdp::DevTables **full);
+// One residue pass of L lanes on stream s.  With span_stream (and fork /
+// join events) given, a pass of more than 8 lanes sweeps its second lane span
+// on that stream, concurrently with the first on s.
 fdp_status fdp_enqueue_pass(fdp_ctx *c, const fdp::DevTables &t, int L, const uint32_t *mods, uint32_t *main,
                             uint32_t *blk, unsigned long long *acc, uint32_t *d_res, uint32_t *h_res,
-                            unsigned int *d_err, cudaStream_t s, uint64_t *launches);
+                            unsigned int *d_err, cudaStream_t s, uint64_t *launches,
+                            cudaStream_t span_stream = nullptr, cudaEvent_t fork = nullptr,
+                            cudaEvent_t join = nullptr);
 // A computation's error word: a kernel that gives up on a bounded wait writes
 // a nonzero value to it.  Each computation (a run_sync graph, one problem of a
 // run_multi_sync graph, one served request) owns its word in its own buffers;

@@ -39,6 +39,8 @@ struct LaunchCfg {
   int row_init = 0;          // strip rows filled directly by the row-k initialiser (0: automatic, -1: never)
   bool row_init_tensor = true;  // the initialiser's products on the tensor cores (else the CUDA cores)
   int split_spans_min_p = 1;    // cells p >= this run each span of a several-span lane count as its own launch
+  bool span_chains = true;  // with every cell split, each span's row sweeps run as a chain of launches of
+                            // their own, concurrent with the other span's (n=22, 14 lanes: pass 17.20 -> 16.83 s)
 };
 
 template <typename Idx, int K>

@@ -151,6 +151,9 @@ fdp_status fdp_run_multi_sync(fdp_ctx *ctx, const fdp_problem *problems, int cou
  * equal, the lanes are independent vectors under one modulus, the GROUPBATCH
  * lane semantics (src/cuda/b300/groupbatch_interleaved.cuh).
  * `stream` is a cudaStream_t (0 = the context's stream); the call is async.
+ * `main` and `block` must be aligned to one word of the widest panel: 32
+ * bytes for 8 or more lanes (an 8-lane word is one 256-bit access), 16 for
+ * 4-7, 8 for 2-3 (cudaMalloc gives 256); otherwise FDP_ERR_ARGS.
  */
 fdp_status fdp_apply_cells(fdp_ctx *ctx, int width, int p_hi, int p_lo, int lanes, const uint32_t *moduli,
                            uint32_t *d_main, uint32_t *d_block, void *stream);
@@ -387,7 +390,8 @@ fdp_status fdp_reverse2_apply(fdp_ctx *ctx, int width, int p, int lanes, const u
  * this entry point again after destroying the device's primary context
  * (cudaDeviceReset).  Every call on a device shares the array; each call
  * clears it on `stream` first, but calls that overlap on the GPU race on it
- * and must be serialised.
+ * and must be serialised.  `d_main` has the alignment fdp_apply_cells asks
+ * of it (32 bytes for 8 or more lanes), or the call returns FDP_ERR_ARGS.
  */
 fdp_status fdp_first_row_dot_noalloc(int width, int lanes, const uint32_t *moduli, const uint32_t *d_main,
                                      uint32_t *d_residues, void *stream);

@@ -418,6 +418,12 @@ extern "C" fdp_status fdp_run_sync(fdp_ctx *c, const fdp_problem *pr, uint32_t *
 
 extern "C" fdp_status fdp_apply_cells(fdp_ctx *c, int width, int p_hi, int p_lo, int lanes, const uint32_t *moduli,
                                       uint32_t *d_main, uint32_t *d_block, void *stream) {
+  // Checked first, before anything that needs a context or a device.
+  if (!fdp::panel_aligned(lanes, d_main) || !fdp::panel_aligned(lanes, d_block)) {
+    g_last_error = "apply_cells: d_main and d_block must be aligned to one word of the widest lane panel "
+                   "(32 bytes for 8 or more lanes, 16 for 4-7, 8 for 2-3)";
+    return FDP_ERR_ARGS;
+  }
   if (!c || !moduli || !d_main || !d_block) return FDP_ERR_ARGS;
   if (width < 2 || width > FDP_MAXW || p_lo < 1 || p_hi >= width || p_lo > p_hi || lanes < 1 ||
       lanes > FDP_MAX_LANES) {

@@ -170,6 +170,11 @@ extern "C" fdp_status fdp_first_row_dot_noalloc(int width, int lanes, const uint
     fdp_set_last_error("fdp_first_row_dot_noalloc: null pointer");
     return FDP_ERR_ARGS;
   }
+  if (!fdp::panel_aligned(lanes, d_main)) {
+    fdp_set_last_error("fdp_first_row_dot_noalloc: d_main must be aligned to one word of the widest lane panel "
+                       "(32 bytes for 8 or more lanes, 16 for 4-7, 8 for 2-3)");
+    return FDP_ERR_ARGS;
+  }
   Mods mods{};
   for (int i = 0; i < lanes; ++i) {
     if (moduli[i] < 2) {

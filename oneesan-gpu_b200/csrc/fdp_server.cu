@@ -118,8 +118,8 @@ struct fdp_server {
   fdp_server_config cfg{};
   char *pool = nullptr;
   PoolAlloc alloc;
-  std::vector<cudaStream_t> streams, span_streams;  // per slot; the second for the second lane span
-  std::vector<cudaEvent_t> ev_start, ev_done, span_fork, span_join;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> ev_start, ev_done;
   std::vector<uint32_t *> pinned;  // per slot, kMaxModuliPerRequest residues, then the error word
   std::vector<Job *> slot_job;
   std::deque<uint64_t> queue;
@@ -165,8 +165,7 @@ struct fdp_server {
     for (int done = 0; done < int(mods.size()) && es == FDP_OK; done += j->lanes) {
       const int L = std::min(j->lanes, int(mods.size()) - done);
       es = fdp_enqueue_pass(ctx, *t, L, mods.data() + done, main, blk, acc, dres, pinned[size_t(slot)] + done,
-                            derr, s, &launches, span_streams[size_t(slot)], span_fork[size_t(slot)],
-                            span_join[size_t(slot)]);
+                            derr, s, &launches);
     }
     if (es == FDP_OK) es = fdp_cuda_status(fdp_enqueue_err_read(herr, derr, s), "serve: error word");
     e = cudaStreamEndCapture(s, &g);
@@ -358,22 +357,13 @@ extern "C" fdp_status fdp_server_start(fdp_ctx *c, const fdp_server_config *cfg)
   sv->alloc.reset(cfg->hbm_budget_bytes);
   const size_t S = size_t(cfg->max_active);
   sv->streams.resize(S);
-  sv->span_streams.resize(S);
   sv->ev_start.resize(S);
   sv->ev_done.resize(S);
-  sv->span_fork.resize(S);
-  sv->span_join.resize(S);
   sv->pinned.resize(S);
   sv->slot_job.assign(S, nullptr);
   fdp_status st = FDP_OK;
   for (size_t i = 0; i < S && st == FDP_OK; ++i) {
     st = fdp_cuda_status(cudaStreamCreateWithFlags(&sv->streams[i], cudaStreamNonBlocking), "server stream");
-    if (st == FDP_OK)
-      st = fdp_cuda_status(cudaStreamCreateWithFlags(&sv->span_streams[i], cudaStreamNonBlocking), "server stream");
-    if (st == FDP_OK)
-      st = fdp_cuda_status(cudaEventCreateWithFlags(&sv->span_fork[i], cudaEventDisableTiming), "server event");
-    if (st == FDP_OK)
-      st = fdp_cuda_status(cudaEventCreateWithFlags(&sv->span_join[i], cudaEventDisableTiming), "server event");
     if (st == FDP_OK) st = fdp_cuda_status(cudaEventCreate(&sv->ev_start[i]), "server event");
     if (st == FDP_OK) st = fdp_cuda_status(cudaEventCreate(&sv->ev_done[i]), "server event");
     if (st == FDP_OK)
@@ -383,9 +373,6 @@ extern "C" fdp_status fdp_server_start(fdp_ctx *c, const fdp_server_config *cfg)
   if (st != FDP_OK) {
     for (size_t i = 0; i < S; ++i) {
       if (sv->streams[i]) cudaStreamDestroy(sv->streams[i]);
-      if (sv->span_streams[i]) cudaStreamDestroy(sv->span_streams[i]);
-      if (sv->span_fork[i]) cudaEventDestroy(sv->span_fork[i]);
-      if (sv->span_join[i]) cudaEventDestroy(sv->span_join[i]);
       if (sv->ev_start[i]) cudaEventDestroy(sv->ev_start[i]);
       if (sv->ev_done[i]) cudaEventDestroy(sv->ev_done[i]);
       if (sv->pinned[i]) cudaFreeHost(sv->pinned[i]);
@@ -411,11 +398,7 @@ void fdp_server_shutdown(fdp_ctx *c) {
   cudaSetDevice(c->device);
   for (size_t i = 0; i < sv->streams.size(); ++i) {
     cudaStreamSynchronize(sv->streams[i]);
-    cudaStreamSynchronize(sv->span_streams[i]);
     cudaStreamDestroy(sv->streams[i]);
-    cudaStreamDestroy(sv->span_streams[i]);
-    cudaEventDestroy(sv->span_fork[i]);
-    cudaEventDestroy(sv->span_join[i]);
     cudaEventDestroy(sv->ev_start[i]);
     cudaEventDestroy(sv->ev_done[i]);
     cudaFreeHost(sv->pinned[i]);

@@ -100,3 +100,27 @@ def test_lane_panels_and_spans():
         assert all(any(p == s for p, _ in panels) for s, _ in spans)  # spans start on a panel
     assert fdp.lane_spans(14) == [(0, 8), (8, 14)]
     assert fdp.lane_spans(8) == [(0, 8)] and fdp.lane_spans(6) == [(0, 6)]
+
+
+def test_misaligned_panel_pointers_are_rejected_on_the_host():
+    # An 8-lane panel word is one 256-bit access, so caller-owned state must be
+    # aligned to one word of the widest panel.  The check runs before anything
+    # that needs a context or a device: these pointers are never dereferenced.
+    import ctypes
+    lib = fdp.lib()
+    apply_cells = lib.fdp_apply_cells
+    noalloc = lib.fdp_first_row_dot_noalloc
+    noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32), ctypes.c_void_p,
+                        ctypes.c_void_p, ctypes.c_void_p]
+    noalloc.restype = ctypes.c_int
+
+    def mods(k):
+        return (ctypes.c_uint32 * k)(*([4294967291] * k))
+
+    for lanes, main, blk in ((8, 0x10010, 0x10000), (14, 0x10000, 0x10010), (16, 0x10008, 0x10000),
+                             (4, 0x10000, 0x10008), (7, 0x10004, 0x10000), (2, 0x10004, 0x10000)):
+        assert apply_cells(None, 13, 12, 1, lanes, mods(lanes), main, blk, None) == fdp.FDP_ERR_ARGS
+        assert b"aligned" in lib.fdp_last_error()
+    for lanes, main in ((8, 0x10010), (16, 0x10008), (5, 0x10008), (3, 0x10004)):
+        assert noalloc(13, lanes, mods(lanes), main, 0x20000, None) == fdp.FDP_ERR_ARGS
+        assert b"aligned" in lib.fdp_last_error()

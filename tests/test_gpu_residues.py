@@ -44,10 +44,12 @@ def test_published_residues(engine, n, mod, want):
 
 
 def test_lane_counts_agree(engine):
+    # Above 8 lanes a pass sweeps its two lane spans as concurrent launch
+    # chains: 9 = {0-7} + {8}, 14 = {0-7} + {8-13}, 16 = {0-7} + {8-15}.
     n = 13
     mods = P[:16]
     plain = engine.residues(n, mods, lanes=1).residues
-    for lanes in (2, 5, 7, 16):
+    for lanes in (2, 5, 7, 9, 14, 16):
         assert engine.residues(n, mods, lanes=lanes).residues == plain
     assert plain[0] == orc.residue(n, mods[0])
 
